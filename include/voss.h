@@ -1,0 +1,213 @@
+/*
+ * voss.h — C ABI of the B200-native VOSS sieve-and-gap engine (libvoss.so).
+ *
+ * The reference (atafhamada/voss-prime-gaps_v1) has no library interface: its hot
+ * path is the stand-alone program src/voss_v7_live.cu, configured by regex-patched
+ * compile-time constants (src/voss_master.py:64-85) and reporting through CSV files
+ * and stdout, plus the verifier program src/verify_cpp.cpp driven by argv.  Each
+ * entry point below replaces one of those interfaces; the comment on each names the
+ * reference lines it stands in for.
+ *
+ * Conventions
+ *   - every function returns int: VOSS_OK (0) or a negative VOSS_ERR_* code; the
+ *     library never calls exit() (the reference exits via CUDA_CHECK,
+ *     src/voss_v7_live.cu:17-21, and on MAX_POS overflow, :516-519);
+ *   - voss_last_error() gives a message for the last failure on this thread;
+ *   - all pointers in signatures are HOST pointers owned by the caller, except the
+ *     *_device entry points, which say so; no pointer is retained after return;
+ *   - integer ranges are half-open [lo, hi); the reference's N-inclusive range
+ *     [1, N] (src/voss_v7_live.cu:435-445) is lo = 1, hi = N + 1;
+ *   - a context is bound to one CUDA device and is used by one host thread at a
+ *     time; use one context per thread.
+ */
+#ifndef VOSS_H
+#define VOSS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define VOSS_API __attribute__((visibility("default")))
+#else
+#define VOSS_API
+#endif
+
+/* ---- error codes ---------------------------------------------------------- */
+#define VOSS_OK 0
+#define VOSS_ERR_ARG (-1)      /* invalid argument */
+#define VOSS_ERR_CUDA (-2)     /* a CUDA runtime call failed */
+#define VOSS_ERR_NOMEM (-3)    /* device or host allocation failed */
+#define VOSS_ERR_RANGE (-4)    /* hi beyond the context's base-prime limit */
+#define VOSS_ERR_DEVICE (-5)   /* a kernel raised its error word */
+#define VOSS_ERR_TIMEOUT (-6)  /* a bounded wait ran out */
+#define VOSS_ERR_STOPPED (-7)  /* stop file seen; checkpoint written */
+#define VOSS_ERR_IO (-8)       /* file could not be read or written */
+#define VOSS_ERR_STATE (-9)    /* object in the wrong state for the call */
+#define VOSS_ERR_NODEV (-10)   /* no CUDA device */
+
+/* ---- sizes shared with the reference's artifact formats ------------------- */
+#define VOSS_MAX_GAP 100000    /* gap histogram covers 0 < g < 1e5: voss_v7_live.cu:23,280 */
+#define VOSS_MODQ_MAX_GAP 100  /* per-residue gap histogram: g < 100: voss_v7_live.cu:25,283 */
+#define VOSS_MODQ_ROWS 10      /* rows: q=6 residues {1,5}, then q=30 residues W30: :26-31,758-764 */
+#define VOSS_NUM_Q 10          /* moduli of voss_range_stats.modq, see VOSS_Q_LIST */
+#define VOSS_MODQ_SLOTS 99     /* 3+4+5+6+7+8+11+12+13+30 */
+#define VOSS_Q_LIST {3, 4, 5, 6, 7, 8, 11, 12, 13, 30}
+#define VOSS_IHIST 1024        /* per-interval gap bins: bin g/2 holds gap g (bin 0 holds g = 1) */
+
+/* voss_range_stats.flags */
+#define VOSS_FLAG_REF_COMPAT 1u /* reproduce voss_v7_live's artifact rules exactly (see below) */
+
+/* One large gap, layout of `struct LargeGap` (src/voss_v7_live.cu:40): position is the
+ * upper prime p_after, merit = (float)(gap / log(p_before)) computed in double. */
+typedef struct voss_large_gap {
+  uint64_t position;
+  int32_t gap;
+  float merit;
+} voss_large_gap;
+
+/*
+ * Whole-range statistics: every array the reference accumulates for its CSVs
+ * (src/voss_v7_live.cu:403-405, 581-594, 634-635, 737-771).
+ *
+ * Full mode (flags = 0): every quantity covers exactly the primes in [lo, hi):
+ *   prime_count, gap_hist over consecutive pairs inside the range, mod4 and modq over
+ *   all primes in range; modq_gap and the large-gap list over pairs whose lower prime
+ *   is >= 7 (the rows of modq_gap are residues coprime to 30).
+ * Reference-compat mode (VOSS_FLAG_REF_COMPAT, lo must be 1): the numbers voss_v7_live
+ *   prints and writes for N = hi - 1 with segment length seg_num:
+ *   - 2, 3, 5 are counted in prime_count, gap_hist (gaps 1, 2 and the 5->7 gap) and
+ *     mod4 (3 and 5), but not in modq, modq_gap or the large-gap list (:404,634-635,682);
+ *   - a gap between primes in different segments [s*seg_num+1, (s+1)*seg_num] enters
+ *     gap_hist only, not modq_gap nor the large-gap list (:559-562).
+ */
+typedef struct voss_range_stats {
+  uint64_t lo, hi;          /* [lo, hi) */
+  uint32_t flags;           /* VOSS_FLAG_* used */
+  uint32_t reserved0;
+  uint64_t seg_num;         /* compat segment length (integers), 0 in full mode */
+  uint64_t prime_count;     /* pi(hi-1) - pi(lo-1); "Total primes" (:639) */
+  uint64_t first_prime;     /* 0 if no prime in range */
+  uint64_t last_prime;      /* 0 if no prime in range; "p_last" (:700) */
+  uint64_t max_gap;         /* largest gap between consecutive primes in range */
+  uint64_t max_gap_lo;      /* lower prime of the first maximal gap */
+  uint64_t mod4[2];         /* [0] = #p = 1 mod 4, [1] = #p = 3 mod 4: pi(x;4,1), pi(x;4,3) (:682) */
+  uint64_t modq[VOSS_MODQ_SLOTS]; /* counts by (q, p mod q), q in VOSS_Q_LIST, q-major */
+  uint64_t modq_gap[VOSS_MODQ_ROWS][VOSS_MODQ_MAX_GAP]; /* [row][gap] (:758-771) */
+  uint64_t large_total;     /* large gaps found (may exceed the caller's capacity) */
+  uint64_t gap_hist[VOSS_MAX_GAP]; /* gaps_total[g] (:403,583,634-635) */
+} voss_range_stats;
+
+/* Per-interval statistics of a batched or served interval query. */
+typedef struct voss_interval_stats {
+  uint64_t lo, hi;          /* [lo, hi) */
+  uint64_t prime_count;
+  uint64_t first_prime, last_prime;   /* 0 if none */
+  uint64_t max_gap, max_gap_lo;       /* 0 if fewer than two primes */
+  uint64_t gap_overflow;              /* gaps >= 2*VOSS_IHIST (none exist below 2^64) */
+  uint64_t gap_hist[VOSS_IHIST];      /* bin g/2 = #gaps of length g; bin 0 = #gaps of length 1 */
+} voss_interval_stats;
+
+/* Sieve tuning; zero fields take the library's defaults. */
+typedef struct voss_tuning {
+  uint32_t block_threads;   /* 512 or 1024 */
+  uint32_t chunk_words;     /* odd; a tile is block_threads * chunk_words 32-bit words */
+  uint32_t ctas_per_sm;     /* resident tiles per SM */
+  uint32_t coop_div;        /* primes p < tile_bytes/coop_div are cleared warp-cooperatively */
+  uint32_t mult_factor;     /* primes p >= mult_factor*tile_bytes use the multiples walk */
+  uint32_t reserved[3];
+} voss_tuning;
+
+typedef struct voss_ctx voss_ctx;
+
+/* ---- library / context ---------------------------------------------------- */
+VOSS_API const char* voss_version(void);
+VOSS_API const char* voss_last_error(void);
+VOSS_API int voss_device_count(int* count);
+
+/* Create a context on `device` able to sieve up to hi = max_hi: builds the base primes
+ * 7 <= p <= isqrt(max_hi - 1) and keeps them resident on the device.
+ * Replaces generate_base_primes + modinv caching (src/voss_v7_live.cu:96-118,357-360,427-431). */
+VOSS_API int voss_ctx_create(int device, uint64_t max_hi, voss_ctx** out);
+VOSS_API void voss_ctx_destroy(voss_ctx* ctx);
+VOSS_API int voss_ctx_info(const voss_ctx* ctx, uint64_t* max_hi, uint64_t* n_base_primes,
+                           int* sm_count);
+VOSS_API int voss_ctx_set_tuning(voss_ctx* ctx, const voss_tuning* t);
+VOSS_API int voss_ctx_get_tuning(const voss_ctx* ctx, voss_tuning* t);
+
+/* ---- single-range sieve + statistics -------------------------------------- */
+/* Sieve [lo, hi) on the device and fill `stats`; the large gaps (gap >= 500 or merit >= 10,
+ * merit computed only for gap > 100: src/voss_v7_live.cu:289-299) go to `large`, up to
+ * large_cap entries, in ascending position order; *large_written receives the count written.
+ * Replaces the segment loop of voss_v7_live main() (:434-626) together with the
+ * accumulation of its epilogue (:634-635,682); the artifacts are written by
+ * voss_write_artifacts.  seg_num is used in REF_COMPAT mode only (must be a multiple of 30). */
+VOSS_API int voss_sieve_range(voss_ctx* ctx, uint64_t lo, uint64_t hi, uint32_t flags,
+                              uint64_t seg_num, voss_range_stats* stats,
+                              voss_large_gap* large, uint64_t large_cap,
+                              uint64_t* large_written);
+
+/* Device-resident form of voss_sieve_range for timing: runs the same kernels on the
+ * context's stream (`stream` = cudaStream_t or NULL for the context's own) and leaves the
+ * results in device memory; voss_fetch_range copies them out and finishes the statistics. */
+VOSS_API int voss_sieve_range_device(voss_ctx* ctx, uint64_t lo, uint64_t hi, uint32_t flags,
+                                     uint64_t seg_num, void* stream);
+VOSS_API int voss_fetch_range(voss_ctx* ctx, voss_range_stats* stats, voss_large_gap* large,
+                              uint64_t large_cap, uint64_t* large_written);
+
+/* Write the primes of [lo, hi) in ascending order to out[0..cap); *count receives the
+ * number of primes in range (out holds min(count, cap) of them).  No counterpart in the
+ * reference beyond its internal positions[] array (src/voss_v7_live.cu:145-179,522-523). */
+VOSS_API int voss_primes_range(voss_ctx* ctx, uint64_t lo, uint64_t hi, uint64_t* out,
+                               uint64_t cap, uint64_t* count);
+
+/* ---- batched intervals ----------------------------------------------------- */
+/* Sieve n independent intervals [lo[i], hi[i]) in one persistent launch over an
+ * (interval, tile) work queue and fill out[i].  The reference has no interval API; each
+ * result equals a one-interval call on the same range. */
+VOSS_API int voss_sieve_intervals(voss_ctx* ctx, const uint64_t* lo, const uint64_t* hi,
+                                  uint32_t n, voss_interval_stats* out);
+
+/* ---- Miller-Rabin and gap proofs -------------------------------------------- */
+/* is_prime[i] = is_prime_u64(n[i]) of src/verify_cpp.cpp:38-57 (12 bases 2..37). */
+VOSS_API int voss_mr_verify(voss_ctx* ctx, const uint64_t* n, uint64_t count, uint8_t* is_prime);
+/* Device pointers; `stream` as for voss_sieve_range_device. */
+VOSS_API int voss_mr_verify_device(voss_ctx* ctx, const uint64_t* d_n, uint64_t count,
+                                   uint8_t* d_is_prime, void* stream);
+/* ok[i] = verify_gap(p_after[i], gap[i]) of src/verify_cpp.cpp:59-93: both ends prime and
+ * every interior integer marked by the reference's interval sieve. */
+VOSS_API int voss_prove_gaps(voss_ctx* ctx, const uint64_t* p_after, const int32_t* gap,
+                             uint64_t count, uint8_t* ok);
+
+/* ---- artifacts --------------------------------------------------------------- */
+/* Write gap_histogram.csv, hl_trend.csv, modq_counts.csv, modq_gap_hist.csv,
+ * chebyshev.csv and large_gaps.csv into `dir` in the byte format of
+ * src/voss_v7_live.cu:707-827 (large gaps sorted by merit, descending, ties by position).
+ * `stats` must come from a REF_COMPAT call with lo = 1. */
+VOSS_API int voss_write_artifacts(const voss_range_stats* stats, const voss_large_gap* large,
+                                  uint64_t n_large, const char* dir);
+
+/* Combine the statistics of adjacent ranges parts[0..n) (parts[i].hi == parts[i+1].lo, same
+ * flags and seg_num) into one, adding the gaps between neighbouring parts: the host half of
+ * a range sharded across GPUs.  large_* describe the concatenated large-gap lists; the
+ * boundary gaps that qualify are appended to large[] up to large_cap. */
+VOSS_API int voss_stats_merge(const voss_range_stats* parts, uint32_t n, voss_range_stats* out,
+                              voss_large_gap* large, uint64_t n_large, uint64_t large_cap,
+                              uint64_t* large_written);
+
+/* ---- diagnostics --------------------------------------------------------------- */
+/* Shared-memory read-modify-write bandwidth of this device (GB/s, 8 bytes per 32-bit
+ * atomicAnd), measured by a bank-conflict-free kernel: the roofline denominator of the
+ * shared-memory-bound sieve.  No counterpart in the reference. */
+VOSS_API int voss_probe_smem_rmw(voss_ctx* ctx, double* gbs);
+/* Kernel time (ms) of the last voss_sieve_range / _device call's sieve kernel, by CUDA events. */
+VOSS_API int voss_last_kernel_ms(const voss_ctx* ctx, double* sieve_ms, double* total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VOSS_H */

@@ -1,0 +1,60 @@
+"""GPU Miller-Rabin and gap proofs against the reference verifier compiled unmodified
+(oracle/_ref/libref_verify.so) and the oracle restatement.  Exact (bool) comparison."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+SPECIAL = [0, 1, 2, 3, 4, 5, 9, 25, 37, 41, 43, 1369, 2047, 3215031751, 341550071728321,
+           3825123056546413051, 18446744073709551557, 18446744073709551615, 18446744073709551614,
+           2**61 - 1, 2**63 - 25, 2**64 - 59, 1000000007, 999999999989, 4759123141, 1122004669633]
+
+
+def checker(n):
+    import os
+    if os.path.exists(O.REF_VERIFY_SO):
+        return O.ref_mr_batch(n)
+    return O.mr_batch(n)
+
+
+def test_mr_special_values(gpu_ctx):
+    n = np.array(SPECIAL, dtype=np.uint64)
+    np.testing.assert_array_equal(gpu_ctx.mr_verify(n), checker(n))
+
+
+def test_mr_random_odd_and_primes(gpu_ctx):
+    rng = np.random.default_rng(20261203)
+    r = rng.integers(0, 2**63, size=200_000, dtype=np.uint64) * 2 + 1
+    p = gpu_ctx.primes_range(10**12 - 3 * 10**6, 10**12)
+    n = np.concatenate([r, p, p + 2, (p[:1000] * p[1:1001]).astype(np.uint64)])
+    got = gpu_ctx.mr_verify(n)
+    np.testing.assert_array_equal(got, checker(n))
+    assert got[r.size:r.size + p.size].all()
+
+
+def test_mr_strong_pseudoprimes(gpu_ctx):
+    # products of two primes p*(2p-1) style values that pass a few bases
+    rng = np.random.default_rng(1)
+    q = gpu_ctx.primes_range(10**6, 2 * 10**6)
+    a = rng.choice(q, 5000)
+    b = 2 * a - 1
+    n = (a * b).astype(np.uint64)
+    np.testing.assert_array_equal(gpu_ctx.mr_verify(n), checker(n))
+
+
+def test_prove_gaps(gpu_ctx):
+    r = gpu_ctx.sieve_range(1, 10**10 + 1, compat=True)
+    lg = r.large
+    p = lg["position"].astype(np.uint64)
+    g = lg["gap"].astype(np.int32)
+    # corrupt some: wrong gap, non-prime end, gap 1/0/negative, p_before = 2 cases
+    bad_p = np.concatenate([p[:50], p[:50] + 2, np.array([3, 5, 7, 11, 13, 2, 29, 97], dtype=np.uint64)])
+    bad_g = np.concatenate([g[:50] - 2, g[:50], np.array([1, 3, 4, 2, 2, 0, -3, 8], dtype=np.int32)])
+    P = np.concatenate([p, bad_p])
+    G = np.concatenate([g, bad_g])
+    got = gpu_ctx.prove_gaps(P, G)
+    want = O.ref_prove_gaps(P, G) if __import__("os").path.exists(O.REF_VERIFY_SO) else O.prove_gaps(P, G)
+    np.testing.assert_array_equal(got, want)
+    assert got[: p.size].all()

@@ -1,0 +1,125 @@
+"""GPU parity of the sieve-and-gap kernels (libvoss.so) against the CPU oracle and the
+reference's golden vectors.  Integer work: every comparison is exact."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")))
+SEG = 30_000_000_000
+
+
+def large_key(arr):
+    return sorted((int(p), int(g)) for p, g in zip(arr["position"], arr["gap"]))
+
+
+def assert_range_equal(g, o, check_large=True):
+    for k in ("lo", "hi", "flags", "seg_num", "prime_count", "first_prime", "last_prime", "max_gap",
+              "max_gap_lo", "large_total"):
+        assert getattr(g, k) == getattr(o, k), (k, getattr(g, k), getattr(o, k))
+    np.testing.assert_array_equal(g.mod4, o.mod4)
+    np.testing.assert_array_equal(g.modq, o.modq)
+    np.testing.assert_array_equal(g.modq_gap, o.modq_gap)
+    np.testing.assert_array_equal(g.gap_hist, o.gap_hist)
+    if check_large:
+        assert large_key(g.large) == large_key(o.large)
+        # merits: device log() vs host log() may differ in the last double ulp; as floats they agree
+        gm = {(int(p), int(x)): float(m) for p, x, m in zip(g.large["position"], g.large["gap"], g.large["merit"])}
+        om = {(int(p), int(x)): float(m) for p, x, m in zip(o.large["position"], o.large["gap"], o.large["merit"])}
+        for key, m in om.items():
+            assert abs(gm[key] - m) <= 4e-6 * max(1.0, abs(m)), (key, gm[key], m)
+
+
+@pytest.mark.parametrize("lo,hi", [
+    (0, 0), (0, 1), (0, 2), (0, 3), (2, 3), (3, 8), (1, 8), (5, 6), (7, 8), (1, 100), (1, 1000), (1, 1001),
+    (1, 10**6 + 1), (2, 10**7), (999_999_000, 1_000_001_000), (10**9, 10**9 + 10**7 + 7),
+    (123_456_789, 987_654_321), (10**12 - 10**8, 10**12 + 1),
+])
+def test_range_full_matches_oracle(gpu_ctx, lo, hi):
+    g = gpu_ctx.sieve_range(lo, hi)
+    o = O.sieve_range(lo, hi)
+    assert_range_equal(g, o)
+
+
+@pytest.mark.parametrize("n", [7, 8, 30, 97, 1000, 10**6, 10**8, 10**9])
+def test_compat_matches_oracle(gpu_ctx, n):
+    g = gpu_ctx.sieve_range(1, n + 1, compat=True, seg_num=SEG)
+    o = O.sieve_range(1, n + 1, compat=True, seg_num=SEG)
+    assert_range_equal(g, o)
+
+
+def test_compat_segment_boundary_rule(gpu_ctx):
+    # a short segment length puts reference-segment seams inside and between tiles
+    t = gpu_ctx.tuning()
+    seg = 30 * 4 * t["block_threads"] * t["chunk_words"] * 3 + 30 * 7  # not a tile multiple
+    for n in (10**8, 3 * 10**8 + 11):
+        g = gpu_ctx.sieve_range(1, n + 1, compat=True, seg_num=seg)
+        o = O.sieve_range(1, n + 1, compat=True, seg_num=seg)
+        assert_range_equal(g, o)
+
+
+def test_random_ranges_match_oracle(gpu_ctx):
+    rng = np.random.default_rng(20261203)
+    for _ in range(12):
+        e = rng.uniform(2, 12.5)
+        lo = int(10**e)
+        ln = int(10 ** rng.uniform(0, 6.5))
+        g = gpu_ctx.sieve_range(lo, lo + ln)
+        o = O.sieve_range(lo, lo + ln)
+        assert_range_equal(g, o)
+
+
+def test_golden_pi_and_chebyshev(gpu_ctx):
+    for n in (9, 10, 11):
+        g = gpu_ctx.sieve_range(1, 10**n + 1, compat=True, seg_num=SEG)
+        assert g.prime_count == GOLD["pi_10n"][str(n)]
+        p41, p43 = GOLD["chebyshev"][str(10**n)]
+        assert (int(g.mod4[0]), int(g.mod4[1])) == (p41, p43)
+        # the reference's three self-checks (src/voss_v7_live.cu:693-705)
+        gh = g.gap_hist
+        assert int(gh.sum()) == g.prime_count - 1
+        assert int((np.arange(gh.size, dtype=np.uint64) * gh).sum()) == g.last_prime - 2
+        assert int(g.mod4.sum()) + 1 == g.prime_count
+
+
+@pytest.mark.parametrize("n", [10**11, 10**12])
+def test_golden_gap_histogram(gpu_ctx, n):
+    g = gpu_ctx.sieve_range(1, n + 1, compat=True, seg_num=SEG)
+    gold = GOLD["gap_hist"][str(n)]
+    got = {str(i): int(c) for i, c in enumerate(g.gap_hist) if c}
+    assert got == gold
+    assert g.prime_count == GOLD["pi_10n"][str(len(str(n)) - 1)]
+    assert [int(g.mod4[0]), int(g.mod4[1])] == GOLD["chebyshev"][str(n)]
+
+
+def test_intervals_match_oracle_and_single_launch(gpu_ctx):
+    rng = np.random.default_rng(7)
+    k = 64
+    lo = (10 ** rng.uniform(1, 12.5, k)).astype(np.uint64)
+    ln = (10 ** rng.uniform(0, 6, k)).astype(np.uint64)
+    lo[:4] = [0, 1, 2, 5]
+    ln[:4] = [0, 30, 1, 1000]
+    hi = lo + ln
+    g = gpu_ctx.sieve_intervals(lo, hi)
+    o = O.sieve_intervals(lo, hi)
+    for f in ("lo", "hi", "prime_count", "first_prime", "last_prime", "max_gap", "max_gap_lo", "gap_overflow"):
+        np.testing.assert_array_equal(g[f], o[f], err_msg=f)
+    np.testing.assert_array_equal(g["gap_hist"], o["gap_hist"])
+    # one plain launch per interval gives the same answers
+    for i in range(0, k, 9):
+        s = gpu_ctx.sieve_intervals(lo[i:i + 1], hi[i:i + 1])
+        for f in ("prime_count", "first_prime", "last_prime", "max_gap", "max_gap_lo"):
+            assert s[f][0] == g[f][i]
+        np.testing.assert_array_equal(s["gap_hist"][0], g["gap_hist"][i])
+
+
+def test_primes_range_matches_oracle(gpu_ctx):
+    for lo, hi in [(0, 100), (1, 10**6), (10**9, 10**9 + 3 * 10**6), (10**12 - 10**6, 10**12)]:
+        g = gpu_ctx.primes_range(lo, hi)
+        o = O.primes_range(lo, hi)
+        np.testing.assert_array_equal(g, o)

@@ -1,0 +1,281 @@
+// mr_kernels.cu — deterministic Miller-Rabin and gap proofs on sm_100a.
+//
+// Result-for-result equal to the reference verifier src/verify_cpp.cpp:
+//   is_prime_u64 (:38-57): n < 2 -> composite; for each base B in {2,...,37}: n == B -> prime,
+//   B | n -> composite; then the strong-probable-prime test to every base.
+//   verify_gap (:59-93): both ends prime, then every interior integer must be marked by the
+//   interval sieve (evens, then odd multiples of the odd base primes q <= isqrt(p_after)).
+//
+// Arithmetic: 64-bit Montgomery multiplication with R = 2^64 (mul.lo/mul.hi on the integer
+// pipe, no 128-bit division); the reference's u128 '%' (verify_cpp.cpp:24) is not used.
+// Base 2 is special-cased: its square-and-multiply multiplies by 2 with a modular addition.
+// Work is split in two kernels so that warps stay full: mr_sieve_kernel resolves every
+// candidate that trial division or base 2 decides (nearly all composites) and appends the rest
+// to a work list; mr_finish_kernel runs the remaining eleven bases on that list.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "voss_internal.h"
+
+namespace voss {
+
+__constant__ uint64_t c_base_inv[12];  // B^-1 mod 2^64 (odd B), for the divisibility test
+__constant__ uint64_t c_base_lim[12];  // floor((2^64-1)/B)
+
+static bool g_mr_ready = false;
+static const uint64_t kBases[12] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+
+struct Mont {
+  uint64_t n, ninv, one, mone;
+};
+
+__device__ __forceinline__ uint64_t mont_mul(uint64_t a, uint64_t b, const Mont& M) {
+  const uint64_t lo = a * b;
+  const uint64_t hi = __umul64hi(a, b);
+  const uint64_t m = lo * M.ninv;
+  const uint64_t mh = __umul64hi(m, M.n);
+  // (a*b + m*n) / 2^64 = hi + mh + carry, carry = (lo != 0) because lo + (m*n mod 2^64) = 0 mod 2^64
+  const uint64_t t = hi + mh;
+  const bool c1 = t < hi;
+  const uint64_t t2 = t + (lo != 0 ? 1ull : 0ull);
+  const bool c2 = t2 < t;
+  return (c1 || c2 || t2 >= M.n) ? t2 - M.n : t2;
+}
+
+__device__ __forceinline__ uint64_t mod_add(uint64_t a, uint64_t b, uint64_t n) {
+  const uint64_t s = a + b;
+  return (s < a || s >= n) ? s - n : s;
+}
+
+__device__ __forceinline__ Mont mont_setup(uint64_t n) {
+  Mont M;
+  M.n = n;
+  uint64_t x = n;  // inverse of n mod 2^3
+#pragma unroll
+  for (int i = 0; i < 5; ++i) x *= 2ull - n * x;
+  M.ninv = 0ull - x;
+  M.one = (0ull - n) % n;  // 2^64 mod n
+  M.mone = n - M.one;
+  return M;
+}
+
+// Trial phase of is_prime_u64: 1 = prime, 0 = composite, -1 = undecided.
+__device__ __forceinline__ int trial_phase(uint64_t n) {
+  if (n < 2) return 0;
+  if (n == 2) return 1;
+  if ((n & 1ull) == 0) return 0;
+#pragma unroll
+  for (int i = 1; i < 12; ++i) {
+    const uint64_t B = i == 1 ? 3 : i == 2 ? 5 : i == 3 ? 7 : i == 4 ? 11 : i == 5 ? 13 : i == 6 ? 17
+                     : i == 7 ? 19 : i == 8 ? 23 : i == 9 ? 29 : i == 10 ? 31 : 37;
+    if (n == B) return 1;
+    if (n * c_base_inv[i] <= c_base_lim[i]) return 0;
+  }
+  return -1;
+}
+
+// Strong probable-prime test of odd n > 37 to the base whose Montgomery form is am.
+__device__ __forceinline__ bool sprp(const Mont& M, uint64_t am, uint64_t d, int r) {
+  uint64_t x = M.one;
+  const int top = 63 - __clzll(d);
+  for (int b = top; b >= 0; --b) {
+    x = mont_mul(x, x, M);
+    if ((d >> b) & 1ull) x = mont_mul(x, am, M);
+  }
+  if (x == M.one || x == M.mone) return true;
+  for (int j = 0; j < r - 1; ++j) {
+    x = mont_mul(x, x, M);
+    if (x == M.mone) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ bool sprp2(const Mont& M, uint64_t d, int r) {
+  uint64_t x = M.one;
+  const int top = 63 - __clzll(d);
+  for (int b = top; b >= 0; --b) {
+    x = mont_mul(x, x, M);
+    if ((d >> b) & 1ull) x = mod_add(x, x, M.n);
+  }
+  if (x == M.one || x == M.mone) return true;
+  for (int j = 0; j < r - 1; ++j) {
+    x = mont_mul(x, x, M);
+    if (x == M.mone) return true;
+  }
+  return false;
+}
+
+// Bases 3..37 (Montgomery forms built from R by modular additions).
+__device__ __forceinline__ bool sprp_rest(const Mont& M, uint64_t d, int r) {
+  const uint64_t n = M.n;
+  const uint64_t r1 = M.one, r2 = mod_add(r1, r1, n), r4 = mod_add(r2, r2, n), r6 = mod_add(r4, r2, n);
+  uint64_t a = mod_add(r2, r1, n);  // 3R
+  // gaps between consecutive bases 3,5,7,11,13,17,19,23,29,31,37
+  const int steps[10] = {2, 2, 4, 2, 4, 2, 4, 6, 2, 6};
+  if (!sprp(M, a, d, r)) return false;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const int s = steps[i];
+    a = mod_add(a, s == 2 ? r2 : (s == 4 ? r4 : r6), n);
+    if (!sprp(M, a, d, r)) return false;
+  }
+  return true;
+}
+
+__device__ bool is_prime_u64_dev(uint64_t n) {
+  const int t = trial_phase(n);
+  if (t >= 0) return t == 1;
+  const Mont M = mont_setup(n);
+  uint64_t d = n - 1;
+  const int r = __ffsll((long long)d) - 1;
+  d >>= r;
+  if (!sprp2(M, d, r)) return false;
+  return sprp_rest(M, d, r);
+}
+
+__global__ void mr_sieve_kernel(const uint64_t* __restrict__ cand, uint64_t count,
+                                uint8_t* __restrict__ out, uint32_t* __restrict__ work,
+                                uint32_t* __restrict__ nwork) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < count; base += stride) {
+    const uint64_t i = base + threadIdx.x;
+    bool need = false;
+    if (i < count) {
+      const uint64_t n = cand[i];
+      const int t = trial_phase(n);
+      if (t >= 0) {
+        out[i] = (uint8_t)t;
+      } else {
+        const Mont M = mont_setup(n);
+        uint64_t d = n - 1;
+        const int r = __ffsll((long long)d) - 1;
+        d >>= r;
+        if (!sprp2(M, d, r)) out[i] = 0;
+        else need = true;
+      }
+    }
+    const unsigned mask = __ballot_sync(0xFFFFFFFFu, need);
+    if (mask) {
+      const int lane = threadIdx.x & 31;
+      uint32_t slot = 0;
+      if (lane == 0) slot = atomicAdd(nwork, (uint32_t)__popc(mask));
+      slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+      if (need) work[slot + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)i;
+    }
+  }
+}
+
+// `work` holds indices < 2^32; candidates beyond that are handled by mr_direct_kernel.
+__global__ void mr_finish_kernel(const uint64_t* __restrict__ cand, uint8_t* __restrict__ out,
+                                 const uint32_t* __restrict__ work, const uint32_t* __restrict__ nwork) {
+  const uint32_t nw = *nwork;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nw; k += gridDim.x * blockDim.x) {
+    const uint32_t i = work[k];
+    const uint64_t n = cand[i];
+    const Mont M = mont_setup(n);
+    uint64_t d = n - 1;
+    const int r = __ffsll((long long)d) - 1;
+    d >>= r;
+    out[i] = sprp_rest(M, d, r) ? 1 : 0;
+  }
+}
+
+// Gap proofs: one warp per gap.  Interior integers are split over the lanes; an interior odd
+// integer is marked by the reference's sieve iff it has an odd prime factor q <= isqrt(p_after),
+// i.e. iff it is composite or itself a prime <= isqrt(p_after).
+__device__ __forceinline__ uint64_t isqrt64(uint64_t x) {
+  uint64_t s = (uint64_t)sqrt((double)x);
+  if (s > 0xFFFFFFFFull) s = 0xFFFFFFFFull;
+  while (s * s > x) --s;
+  while (s < 0xFFFFFFFFull && (s + 1) * (s + 1) <= x) ++s;
+  return s;
+}
+
+__global__ void prove_gaps_kernel(const uint64_t* __restrict__ p_after, const int32_t* __restrict__ gap,
+                                  uint64_t count, uint8_t* __restrict__ ok) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < count; g += warps) {
+    const uint64_t pa = p_after[g];
+    const int32_t gp = gap[g];
+    const uint64_t pb = pa - (uint64_t)(int64_t)gp;
+    bool end_ok = true;
+    if (lane == 0) end_ok = is_prime_u64_dev(pb);
+    if (lane == 1) end_ok = is_prime_u64_dev(pa);
+    const bool ends = __all_sync(0xFFFFFFFFu, end_ok);
+    bool res = ends;
+    if (ends && gp >= 2) {
+      if ((pb & 1ull) == 0) {
+        res = false;  // p_before = 2: the even-index marking leaves interior 4 unmarked
+      } else {
+        const uint64_t sq = isqrt64(pa);
+        const uint64_t n_odd = (uint64_t)(gp - 2) / 2;  // odd integers pb+2 .. pa-2
+        bool bad = false;
+        for (uint64_t k0 = 0; k0 < n_odd; k0 += 32) {
+          const uint64_t k = k0 + lane;
+          bool unmarked = false;
+          if (k < n_odd) {
+            const uint64_t v = pb + 2 + 2 * k;
+            if (v > sq) unmarked = is_prime_u64_dev(v);
+          }
+          if (__any_sync(0xFFFFFFFFu, unmarked)) {
+            bad = true;
+            break;
+          }
+        }
+        res = !bad;
+      }
+    }
+    if (lane == 0) ok[g] = res ? 1 : 0;
+  }
+}
+
+static int ensure_mr_tables() {
+  if (g_mr_ready) return 0;
+  uint64_t inv[12], lim[12];
+  for (int i = 0; i < 12; ++i) {
+    const uint64_t b = kBases[i];
+    uint64_t x = b;
+    if (b & 1) {
+      for (int k = 0; k < 5; ++k) x *= 2ull - b * x;
+    } else {
+      x = 0;
+    }
+    inv[i] = x;
+    lim[i] = ~0ull / b;
+  }
+  if (cudaMemcpyToSymbol(c_base_inv, inv, sizeof(inv)) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(c_base_lim, lim, sizeof(lim)) != cudaSuccess) return -1;
+  g_mr_ready = true;
+  return 0;
+}
+
+int launch_mr(const uint64_t* d_n, uint64_t count, uint8_t* d_out, uint32_t* d_work,
+              uint32_t* d_nwork, void* stream, int sm_count) {
+  if (ensure_mr_tables()) return -1;
+  if (count == 0) return 0;
+  if (count > 0xFFFFFFFFull) return -1;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemsetAsync(d_nwork, 0, sizeof(uint32_t), s) != cudaSuccess) return -1;
+  const int blk = 256;
+  uint64_t want = (count + blk - 1) / blk;
+  int grid = (int)(want < (uint64_t)sm_count * 16 ? want : (uint64_t)sm_count * 16);
+  mr_sieve_kernel<<<grid, blk, 0, s>>>(d_n, count, d_out, d_work, d_nwork);
+  mr_finish_kernel<<<sm_count * 8, blk, 0, s>>>(d_n, d_out, d_work, d_nwork);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_prove_gaps(const uint64_t* d_p_after, const int32_t* d_gap, uint64_t count,
+                      uint8_t* d_ok, void* stream, int sm_count) {
+  if (ensure_mr_tables()) return -1;
+  if (count == 0) return 0;
+  const int blk = 256;
+  const uint64_t warps_needed = count;
+  uint64_t want = (warps_needed + (blk / 32) - 1) / (blk / 32);
+  int grid = (int)(want < (uint64_t)sm_count * 16 ? want : (uint64_t)sm_count * 16);
+  prove_gaps_kernel<<<grid, blk, 0, (cudaStream_t)stream>>>(d_p_after, d_gap, count, d_ok);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace voss

@@ -1,0 +1,830 @@
+// sieve_kernels.cu — the sm_100a sieve-and-gap kernels.
+//
+// One persistent kernel (sieve_tiles_kernel) replaces the reference's per-segment pipeline
+// memset -> graph of one sieve_w30_seg_kernel launch per base prime -> extract -> thrust::sort
+// -> mod4 -> modq -> gaps (src/voss_v7_live.cu:120-312, 480-585).  Each CTA claims tiles of the
+// wheel-30 bitmap from an atomic work counter and, for every tile, entirely in shared memory:
+//   1. fill:     writes the tile pre-sieved by 7..31 from four periodic word-mask tables and
+//                masks the interval's ends (the reference's cudaMemset + first-word patch, :496-500);
+//   2. sieve:    clears the odd multiples of the base primes 37 <= p <= isqrt(hi-1)
+//                (the reference's sieve_w30_seg_kernel, :120-143, one launch per prime):
+//                  small primes  p <  tile_bytes/coop_div : one warp per prime, lanes stride 32p,
+//                  medium primes p <  mult_factor*tile_bytes: one thread per prime, 8 residues,
+//                  large primes  otherwise                 : one thread per prime, walking its
+//                                                            multiples across the tile's span;
+//   3. restore:  sets the bits of base primes lying in the tile (the reference starts each prime
+//                at p^2, :452-466; here the p*1 hit is undone instead);
+//   4. extract:  each thread walks a contiguous chunk of words in order (ffs), its predecessor
+//                prime coming from a block-wide max-scan of the chunks' last primes, and updates
+//                shared-memory counters: the gap histogram (:278-280), the per-residue gap
+//                histogram (:282-287), residue classes for mod-4 and mod-q (:181-232), the
+//                large-gap list (:289-299) and the tile's maximal gap.  Primes never reach HBM.
+// The gaps across tile seams are added by stitch_kernel; reduce_kernel gives each interval its
+// first/last prime and maximal gap.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "voss_internal.h"
+
+namespace voss {
+
+// [bi*8 + o]: for a prime p = 30a + b (b = W30[bi]) and multiplier residue w = W30[o],
+// p*w = 30*(a*w + D) + W30[B] with D = floor(b*w/30), stored as D | (B << 5).
+__constant__ uint8_t c_wheel_step[64];
+// residue r (mod 30) -> wheel bit index, or -1 when gcd(r, 30) > 1.
+__constant__ int8_t c_res_bit[32];
+
+static bool g_tables_ready = false;
+
+__device__ __forceinline__ uint32_t w30(uint32_t o) {
+  return (uint32_t)((kW30Packed >> (8u * o)) & 0xFFu);
+}
+
+// x mod p with m = floor((2^64-1)/p): q <= x/p < q + 3.
+__device__ __forceinline__ uint32_t mod_barrett(uint64_t x, uint32_t p, uint64_t m) {
+  uint64_t q = __umul64hi(x, m);
+  uint64_t r = x - q * (uint64_t)p;
+  if (r >= p) r -= p;
+  if (r >= p) r -= p;
+  return (uint32_t)r;
+}
+
+__device__ __forceinline__ uint64_t isqrt_u64(uint64_t x) {
+  uint64_t s = (uint64_t)sqrt((double)x);
+  if (s > 0xFFFFFFFFull) s = 0xFFFFFFFFull;
+  while (s * s > x) --s;
+  while (s < 0xFFFFFFFFull && (s + 1) * (s + 1) <= x) ++s;
+  return s;
+}
+
+// number of table primes <= v
+__device__ __forceinline__ uint32_t count_le(const uint32_t* pr, uint32_t n, uint64_t v) {
+  if (v >= 0xFFFFFFFFull) return n;
+  uint32_t lo = 0, hi = n, x = (uint32_t)v;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (pr[mid] <= x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// number of table primes < v
+__device__ __forceinline__ uint32_t count_lt(const uint32_t* pr, uint32_t n, uint64_t v) {
+  if (v == 0) return 0;
+  return count_le(pr, n, v - 1);
+}
+
+__device__ __forceinline__ uint32_t find_interval(const SieveArgs& a, uint32_t t) {
+  uint32_t lo = 0, hi = a.n_intervals;  // largest i with tile_begin <= t
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (a.iv[mid].tile_begin <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+#ifdef VOSS_BOUNDS_CHECK
+#define VOSS_SM_GUARD(idx, limit)             \
+  if ((idx) >= (limit)) {                     \
+    atomicOr(err, kErrBounds);                \
+    return;                                   \
+  }
+#else
+#define VOSS_SM_GUARD(idx, limit)
+#endif
+
+__device__ __forceinline__ void clear_bit_word(uint32_t* bm, uint32_t word, uint32_t mask,
+                                               uint32_t limit, uint32_t* err) {
+  VOSS_SM_GUARD(word, limit)
+  atomicAnd(bm + word, mask);
+}
+
+__device__ __forceinline__ void sm_add(uint32_t* cnt, uint32_t idx, uint32_t* err) {
+  VOSS_SM_GUARD(idx, (uint32_t)kSmCounters)
+  atomicAdd(cnt + idx, 1u);
+}
+
+// Mask of the bits of word w whose integers lie in [vlo, vhi); v0 = value of byte 4w, residue 0.
+__device__ __forceinline__ uint32_t edge_mask(uint64_t v0, uint64_t vlo, uint64_t vhi) {
+  uint32_t m = 0;
+#pragma unroll
+  for (uint32_t j = 0; j < 4; ++j)
+#pragma unroll
+    for (uint32_t o = 0; o < 8; ++o) {
+      uint64_t v = v0 + 30u * j + w30(o);
+      if (v >= vlo && v < vhi) m |= 1u << (8u * j + o);
+    }
+  return m;
+}
+
+__device__ __forceinline__ uint32_t pre_mod(int g) {
+  return g == 0 ? 1001u : (g == 1 ? 323u : (g == 2 ? 667u : 31u));
+}
+__device__ __forceinline__ uint32_t pre_off(int g) {
+  return g == 0 ? 0u : (g == 1 ? 1001u : (g == 2 ? 1324u : 1991u));
+}
+
+struct TileHdr {
+  unsigned long long ktile, vbase, vlo, vhi, seg_k;
+  uint32_t nw, lt, np, ia, ib, vb, gthr, k28, k143;
+  uint32_t pre_base[kPreGroups];
+  uint32_t interval, tile, next_tile, cur_iv, since_flush, flush;
+  uint32_t r0, r1;       // base primes lying in the tile (restore)
+  uint32_t coop_ctr;
+  uint32_t first;
+  uint32_t tile_base_rank;
+  unsigned long long count_total;
+};
+
+template <int BLOCK>
+struct BlockScratch {
+  int32_t warp_max[BLOCK / 32];
+  int32_t warp_prefix[BLOCK / 32];
+  int32_t block_max;
+  uint32_t warp_sum[BLOCK / 32];
+  unsigned long long warp_key[BLOCK / 32];
+};
+
+// Exclusive max-scan of `v` over thread order; returns the exclusive prefix and, through
+// *total, the max over the block.
+template <int BLOCK>
+__device__ __forceinline__ int32_t block_excl_max(int32_t v, BlockScratch<BLOCK>& S, int32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int32_t incl = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    int32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+    if (lane >= d) incl = max(incl, t);
+  }
+  if (lane == 31) S.warp_max[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int32_t x = lane < BLOCK / 32 ? S.warp_max[lane] : -1;
+    int32_t y = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      int32_t t = __shfl_up_sync(0xFFFFFFFFu, y, d);
+      if (lane >= d) y = max(y, t);
+    }
+    int32_t ex = __shfl_up_sync(0xFFFFFFFFu, y, 1);
+    if (lane == 0) ex = -1;
+    if (lane < BLOCK / 32) S.warp_prefix[lane] = ex;
+    if (lane == BLOCK / 32 - 1) S.block_max = y;
+  }
+  __syncthreads();
+  int32_t ex = __shfl_up_sync(0xFFFFFFFFu, incl, 1);
+  if (lane == 0) ex = -1;
+  ex = max(ex, S.warp_prefix[warp]);
+  *total = S.block_max;
+  return ex;
+}
+
+template <int BLOCK>
+__device__ __forceinline__ uint32_t block_excl_sum(uint32_t v, BlockScratch<BLOCK>& S, uint32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+    if (lane >= d) incl += t;
+  }
+  if (lane == 31) S.warp_sum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t x = lane < BLOCK / 32 ? S.warp_sum[lane] : 0;
+    uint32_t y = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t t = __shfl_up_sync(0xFFFFFFFFu, y, d);
+      if (lane >= d) y += t;
+    }
+    if (lane < BLOCK / 32) S.warp_sum[lane] = y - x;  // exclusive prefix of warps
+    if (lane == BLOCK / 32 - 1) S.warp_prefix[0] = (int32_t)y;
+  }
+  __syncthreads();
+  uint32_t ex = incl - v + S.warp_sum[warp];
+  *total = (uint32_t)S.warp_prefix[0];
+  return ex;
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void block_reduce_tile(uint32_t cnt, unsigned long long key,
+                                                  BlockScratch<BLOCK>& S, uint32_t* cnt_total,
+                                                  unsigned long long* key_max) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, d);
+    unsigned long long k2 = __shfl_down_sync(0xFFFFFFFFu, key, d);
+    key = k2 > key ? k2 : key;
+  }
+  if (lane == 0) {
+    S.warp_sum[warp] = cnt;
+    S.warp_key[warp] = key;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t c = lane < BLOCK / 32 ? S.warp_sum[lane] : 0;
+    unsigned long long k = lane < BLOCK / 32 ? S.warp_key[lane] : 0ull;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      c += __shfl_down_sync(0xFFFFFFFFu, c, d);
+      unsigned long long k2 = __shfl_down_sync(0xFFFFFFFFu, k, d);
+      k = k2 > k ? k2 : k;
+    }
+    if (lane == 0) {
+      *cnt_total = c;
+      *key_max = k;
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t acc_index(uint32_t i) {
+  return i < (uint32_t)kSmModq ? (uint32_t)kAccHist + i : (uint32_t)kAccModq + (i - (uint32_t)kSmModq);
+}
+
+constexpr uint32_t kFlushEvery = 2048;  // tiles between counter flushes (u32 headroom)
+
+template <int BLOCK, bool EMIT>
+__global__ void __launch_bounds__(BLOCK, (BLOCK == 512 ? 2 : 1))
+sieve_tiles_kernel(SieveArgs a) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* bm = smem;
+  uint32_t* pre = smem + a.tile_words;
+  uint32_t* cnt = pre + kPreWords;
+  __shared__ TileHdr H;
+  __shared__ BlockScratch<BLOCK> S;
+  uint32_t* err = a.error;
+
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (uint32_t i = tid; i < kPreWords; i += BLOCK) pre[i] = a.pretab[i];
+  if (!EMIT)
+    for (uint32_t i = tid; i < (uint32_t)kSmCounters; i += BLOCK) cnt[i] = 0;
+  if (tid == 0) {
+    H.next_tile = atomicAdd(a.tile_counter, 1u);
+    H.cur_iv = kNone;
+    H.since_flush = 0;
+    H.count_total = 0;
+  }
+  __syncthreads();
+
+  const uint32_t C = a.chunk_words;
+
+  for (;;) {
+    // ---- claim / flush ------------------------------------------------------------------
+    if (tid == 0) {
+      uint32_t t = H.next_tile;
+      uint32_t ivx = t < a.n_tiles ? find_interval(a, t) : kNone;
+      H.tile = t;
+      H.interval = ivx;
+      H.flush = (!EMIT && H.cur_iv != kNone &&
+                 (ivx != H.cur_iv || H.since_flush >= kFlushEvery)) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (H.flush) {
+      unsigned long long* acc = a.acc + (size_t)H.cur_iv * kAccStride;
+      for (uint32_t i = tid; i < (uint32_t)kSmCounters; i += BLOCK) {
+        uint32_t v = cnt[i];
+        if (v) {
+          atomicAdd(acc + acc_index(i), (unsigned long long)v);
+          cnt[i] = 0;
+        }
+      }
+      if (tid == 0) {
+        atomicAdd(acc + kAccCount, H.count_total);
+        H.count_total = 0;
+        H.since_flush = 0;
+      }
+      __syncthreads();
+    }
+    if (H.tile >= a.n_tiles) break;
+
+    // ---- tile header ------------------------------------------------------------------
+    if (tid == 0) {
+      const IntervalDev iv = a.iv[H.interval];
+      const uint32_t tl = H.tile - iv.tile_begin;
+      const uint64_t wofs = (uint64_t)tl * a.tile_words;
+      const uint64_t nw64 = iv.n_words - wofs;
+      const uint32_t nw = nw64 < a.tile_words ? (uint32_t)nw64 : a.tile_words;
+      const uint64_t ktile = iv.k0 + 4ull * wofs;
+      H.cur_iv = H.interval;
+      H.ktile = ktile;
+      H.vbase = 30ull * ktile;
+      H.vlo = iv.lo;
+      H.vhi = iv.hi;
+      H.seg_k = iv.seg_k;
+      H.nw = nw;
+      H.lt = 4u * nw;
+      uint64_t vend = H.vbase + 30ull * H.lt;
+      if (vend > iv.hi) vend = iv.hi;
+      const uint32_t np = count_le(a.primes, a.n_primes, isqrt_u64(vend - 1));
+      H.np = np;
+      uint32_t ia = count_lt(a.primes, np, (uint64_t)(H.lt / a.coop_div));
+      uint32_t ib = count_lt(a.primes, np, (uint64_t)H.lt * a.mult_factor);
+      H.ia = ia;
+      H.ib = ib < ia ? ia : ib;
+      H.r0 = count_lt(a.primes, a.n_primes, H.vbase);
+      H.r1 = count_lt(a.primes, a.n_primes, H.vbase + 30ull * H.lt);
+      uint32_t vb = kNone;
+      if (iv.seg_k) {
+        uint64_t kb = (ktile / iv.seg_k + 1) * iv.seg_k;
+        if (kb < ktile + H.lt) vb = (uint32_t)(30ull * (kb - ktile));
+      }
+      H.vb = vb;
+      double lv = log((double)(H.vbase > 7 ? H.vbase : 7));
+      double th = floor(10.0 * lv) - 2.0;
+      H.gthr = th < 0 ? 0u : (th > 1e9 ? 1000000000u : (uint32_t)th);
+      H.k28 = (uint32_t)(ktile % 28ull);
+      H.k143 = (uint32_t)(ktile % 143ull);
+      const uint64_t wt = ktile >> 2;
+#pragma unroll
+      for (int g = 0; g < kPreGroups; ++g) H.pre_base[g] = (uint32_t)(wt % pre_mod(g));
+      H.coop_ctr = 0;
+      H.first = kNone;
+    }
+    __syncthreads();
+
+    const uint32_t nw = H.nw, Lt = H.lt;
+
+    // ---- 1. fill ----------------------------------------------------------------------
+    {
+      uint32_t ix[kPreGroups], st[kPreGroups];
+#pragma unroll
+      for (int g = 0; g < kPreGroups; ++g) {
+        ix[g] = (H.pre_base[g] + (uint32_t)tid) % pre_mod(g);
+        st[g] = (uint32_t)BLOCK % pre_mod(g);
+      }
+      const uint64_t vbase = H.vbase, vlo = H.vlo, vhi = H.vhi;
+      for (uint32_t w = tid; w < a.tile_words; w += BLOCK) {
+        uint32_t m = 0;
+        if (w < nw) {
+          m = pre[ix[0]] & pre[1001u + ix[1]] & pre[1324u + ix[2]] & pre[1991u + ix[3]];
+          const uint64_t v0 = vbase + 120ull * w;
+          if (v0 + 1 < vlo || v0 + 120 > vhi) m &= edge_mask(v0, vlo, vhi);
+        }
+        bm[w] = m;
+#pragma unroll
+        for (int g = 0; g < kPreGroups; ++g) {
+          ix[g] += st[g];
+          if (ix[g] >= pre_mod(g)) ix[g] -= pre_mod(g);
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- 2. sieve ----------------------------------------------------------------------
+    {
+      const uint64_t ktile = H.ktile;
+      const uint32_t ia = H.ia, ib = H.ib, np = H.np;
+      // small primes: a warp per prime
+      for (;;) {
+        uint32_t i = 0;
+        if (lane == 0) i = atomicAdd(&H.coop_ctr, 1u);
+        i = __shfl_sync(0xFFFFFFFFu, i, 0);
+        if (i >= ia) break;
+        const uint32_t p = a.primes[i];
+        const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
+        const uint32_t pa = p / 30u, bi = (uint32_t)c_res_bit[p - 30u * pa];
+        const uint32_t stride = 32u * p;
+#pragma unroll 1
+        for (uint32_t o = 0; o < 8; ++o) {
+          const uint32_t e = c_wheel_step[bi * 8u + o];
+          const uint32_t delta = pa * w30(o) + (e & 31u);
+          uint32_t s = delta >= r ? delta - r : delta + p - r;
+          uint32_t byte = s + (uint32_t)lane * p;
+          const uint32_t mask = ~(1u << (((byte & 3u) << 3) | (e >> 5)));
+          for (; byte < Lt; byte += stride) clear_bit_word(bm, byte >> 2, mask, nw, err);
+        }
+      }
+      // medium primes: a thread per prime, 8 residue progressions
+      for (uint32_t i = ia + tid; i < ib; i += BLOCK) {
+        const uint32_t p = a.primes[i];
+        const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
+        const uint32_t pa = p / 30u, bi = (uint32_t)c_res_bit[p - 30u * pa];
+#pragma unroll
+        for (uint32_t o = 0; o < 8; ++o) {
+          const uint32_t e = c_wheel_step[bi * 8u + o];
+          const uint32_t delta = pa * w30(o) + (e & 31u);
+          uint32_t byte = delta >= r ? delta - r : delta + p - r;
+          const uint32_t bit = e >> 5;
+          for (; byte < Lt; byte += p)
+            clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
+        }
+      }
+      // large primes: walk the multiples of p across the tile's span of integers
+      const uint64_t vbase = H.vbase;
+      const uint32_t span = 30u * Lt;
+      for (uint32_t i = ib + tid; i < np; i += BLOCK) {
+        const uint32_t p = a.primes[i];
+        const uint32_t r = mod_barrett(vbase, p, a.magic[i]);
+        uint32_t d = r ? p - r : 0u;
+        for (; d < span; d += p) {
+          const uint32_t q = d / 30u;
+          const int b = c_res_bit[d - 30u * q];
+          if (b >= 0) clear_bit_word(bm, q >> 2, ~(1u << (((q & 3u) << 3) | (uint32_t)b)), nw, err);
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- 3. restore primes lying in the tile ---------------------------------------------
+    {
+      const uint64_t vbase = H.vbase, vlo = H.vlo, vhi = H.vhi, vend = vbase + 30ull * Lt;
+      if (vbase < 32 && tid < 8) {
+        const uint32_t sp[8] = {7, 11, 13, 17, 19, 23, 29, 31};
+        const uint64_t p = sp[tid];
+        if (p >= vlo && p < vhi && p >= vbase && p < vend) {
+          const uint32_t off = (uint32_t)(p - vbase), k = off / 30u;
+          atomicOr(bm + (k >> 2), 1u << (((k & 3u) << 3) | (uint32_t)c_res_bit[off - 30u * k]));
+        }
+      }
+      for (uint32_t i = H.r0 + tid; i < H.r1; i += BLOCK) {
+        const uint64_t p = a.primes[i];
+        if (p >= vlo && p < vhi && p >= vbase && p < vend) {
+          const uint32_t off = (uint32_t)(p - vbase), k = off / 30u;
+          if ((k >> 2) < nw)
+            atomicOr(bm + (k >> 2), 1u << (((k & 3u) << 3) | (uint32_t)c_res_bit[off - 30u * k]));
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- 4. extract -----------------------------------------------------------------------
+    const uint32_t c0 = (uint32_t)tid * C;
+    const uint32_t cend = c0 < nw ? (c0 + C < nw ? c0 + C : nw) : c0;
+
+    if (EMIT) {
+      uint32_t pc = 0;
+      for (uint32_t w = c0; w < cend; ++w) pc += __popc(bm[w]);
+      uint32_t total;
+      uint32_t rank = block_excl_sum<BLOCK>(pc, S, &total);
+      const unsigned long long base = a.tile_offset[H.tile];
+      const uint64_t vbase = H.vbase;
+      for (uint32_t w = c0; w < cend; ++w) {
+        uint32_t x = bm[w];
+        while (x) {
+          const uint32_t b = (uint32_t)__ffs(x) - 1u;
+          x &= x - 1u;
+          const unsigned long long idx = base + rank;
+          if (idx < a.out_cap) a.out[idx] = vbase + 120ull * w + 30u * (b >> 3) + w30(b & 7u);
+          ++rank;
+        }
+      }
+      __syncthreads();
+    } else {
+      // pass 1: last prime of my chunk
+      int32_t my_last = -1;
+      for (uint32_t w = cend; w > c0;) {
+        --w;
+        const uint32_t x = bm[w];
+        if (x) {
+          const uint32_t b = 31u - (uint32_t)__clz(x);
+          my_last = (int32_t)(120u * w + 30u * (b >> 3) + w30(b & 7u));
+          break;
+        }
+      }
+      int32_t tile_last;
+      int32_t prev = block_excl_max<BLOCK>(my_last, S, &tile_last);
+
+      // pass 2: walk the chunk in order
+      const uint32_t vb = H.vb;
+      const uint32_t gthr = H.gthr;
+      uint32_t k28 = (H.k28 + 4u * c0) % 28u;
+      uint32_t k143 = (H.k143 + 4u * c0) % 143u;
+      uint32_t my_cnt = 0, mg = 0, mlo = 0;
+      uint32_t o_prev = 0;
+      if (prev >= 0) {
+        const uint32_t kp = (uint32_t)prev / 30u;
+        o_prev = (uint32_t)c_res_bit[(uint32_t)prev - 30u * kp];
+      }
+      uint32_t w = c0;
+      uint32_t x = w < cend ? bm[w] : 0u;
+      for (;;) {
+        while (x == 0u) {
+          if (++w >= cend) break;
+          x = bm[w];
+          k28 += 4u;
+          if (k28 >= 28u) k28 -= 28u;
+          k143 += 4u;
+          if (k143 >= 143u) k143 -= 143u;
+        }
+        if (w >= cend) break;
+        const uint32_t b = (uint32_t)__ffs(x) - 1u;
+        x &= x - 1u;
+        const uint32_t j = b >> 3, o = b & 7u;
+        const uint32_t pos = 120u * w + 30u * j + w30(o);
+        ++my_cnt;
+        uint32_t c = k28 + j;
+        if (c >= 28u) c -= 28u;
+        sm_add(cnt, kSmCls28 + c * 8u + o, err);
+        c = k143 + j;
+        if (c >= 143u) c -= 143u;
+        sm_add(cnt, kSmCls143 + c * 8u + o, err);
+        if (prev >= 0) {
+          const uint32_t g = pos - (uint32_t)prev;
+          const bool crossing = ((uint32_t)prev < vb) && (pos >= vb);
+          if (g < 100u && !crossing) {
+            sm_add(cnt, kSmModq + o_prev * kModqBins + (g >> 1), err);
+          } else if (g < 2u * kHistBins) {
+            sm_add(cnt, kSmHist + (g >> 1), err);
+          } else {
+            atomicAdd(a.acc + (size_t)H.cur_iv * kAccStride + kAccHistOver, 1ull);
+            const uint32_t slot = atomicAdd(a.over_count, 1u);
+            if (slot < a.over_cap) a.over[slot] = OverflowGap{H.cur_iv, g};
+            else atomicOr(err, kErrOverflowList);
+          }
+          if (g > mg) {
+            mg = g;
+            mlo = (uint32_t)prev;
+          }
+          if (a.want_large && g > 100u && !crossing && (g >= 500u || g >= gthr)) {
+            const uint64_t v0 = H.vbase + (uint32_t)prev;
+            const double merit_d = (double)g / log((double)v0);
+            if (g >= 500u || merit_d >= 10.0) {
+              const uint32_t slot = atomicAdd(a.large_count, 1u);
+              if (slot < a.large_cap) {
+                a.large[slot] = LargeGapDev{H.vbase + pos, (int32_t)g, (float)merit_d};
+                a.large_iv[slot] = H.cur_iv;
+              }
+            }
+          }
+        } else {
+          H.first = pos;  // exactly one thread meets a prime with no predecessor in the tile
+        }
+        prev = (int32_t)pos;
+        o_prev = o;
+      }
+      const unsigned long long key =
+          mg ? (((unsigned long long)mg << 32) | (unsigned long long)(0xFFFFFFFFu - mlo)) : 0ull;
+      uint32_t tile_cnt;
+      unsigned long long tile_key;
+      __syncthreads();  // H.first visible, scratch reuse
+      block_reduce_tile<BLOCK>(my_cnt, key, S, &tile_cnt, &tile_key);
+      if (tid == 0) {
+        TilePartial P;
+        P.first = tile_cnt ? H.first : kNone;
+        P.last = tile_cnt ? (uint32_t)tile_last : kNone;
+        P.count = tile_cnt;
+        P.max_gap = (uint32_t)(tile_key >> 32);
+        P.max_lo = tile_key ? 0xFFFFFFFFu - (uint32_t)(tile_key & 0xFFFFFFFFull) : 0u;
+        P.bgap = 0;
+        P.bgap_lo = 0;
+        a.partials[H.tile] = P;
+        H.count_total += tile_cnt;
+        H.since_flush++;
+      }
+    }
+    if (tid == 0) H.next_tile = atomicAdd(a.tile_counter, 1u);
+    __syncthreads();
+  }
+}
+
+// Gap between the last prime of the previous non-empty tile and this tile's first prime.
+__global__ void stitch_kernel(SieveArgs a) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n_tiles) return;
+  const TilePartial P = a.partials[t];
+  if (P.count == 0) return;
+  const uint32_t ivx = find_interval(a, t);
+  const IntervalDev iv = a.iv[ivx];
+  uint32_t tp = t;
+  bool found = false;
+  while (tp > iv.tile_begin) {
+    --tp;
+    if (a.partials[tp].count) {
+      found = true;
+      break;
+    }
+  }
+  if (!found) return;
+  const uint64_t kt = iv.k0 + 4ull * a.tile_words * (t - iv.tile_begin);
+  const uint64_t kp = iv.k0 + 4ull * a.tile_words * (tp - iv.tile_begin);
+  const uint64_t hi_p = 30ull * kt + P.first;
+  const uint64_t lo_p = 30ull * kp + a.partials[tp].last;
+  const uint64_t g = hi_p - lo_p;
+  const bool crossing = iv.seg_k && ((lo_p / 30ull) / iv.seg_k != (hi_p / 30ull) / iv.seg_k);
+  unsigned long long* acc = a.acc + (size_t)ivx * kAccStride;
+  if (g < 100 && !crossing) {
+    const uint32_t o_prev = (uint32_t)c_res_bit[lo_p % 30ull];
+    atomicAdd(acc + kAccModq + o_prev * kModqBins + (g >> 1), 1ull);
+  } else if (g < 2ull * kHistBins) {
+    atomicAdd(acc + kAccHist + (g >> 1), 1ull);
+  } else {
+    atomicAdd(acc + kAccHistOver, 1ull);
+    const uint32_t slot = atomicAdd(a.over_count, 1u);
+    if (slot < a.over_cap) a.over[slot] = OverflowGap{ivx, (uint32_t)(g > 0xFFFFFFFFull ? 0xFFFFFFFFull : g)};
+    else atomicOr(a.error, kErrOverflowList);
+  }
+  a.partials[t].bgap = (uint32_t)(g > 0xFFFFFFFFull ? 0xFFFFFFFFull : g);
+  a.partials[t].bgap_lo = lo_p;
+  if (a.want_large && g > 100 && !crossing) {
+    const double merit_d = (double)g / log((double)lo_p);
+    if (g >= 500 || merit_d >= 10.0) {
+      const uint32_t slot = atomicAdd(a.large_count, 1u);
+      if (slot < a.large_cap) {
+        a.large[slot] = LargeGapDev{hi_p, (int32_t)g, (float)merit_d};
+        a.large_iv[slot] = ivx;
+      }
+    }
+  }
+}
+
+// One block per interval: first/last prime and the first maximal gap.
+__global__ void reduce_kernel(SieveArgs a, IntervalOut* out) {
+  const uint32_t ivx = blockIdx.x;
+  if (ivx >= a.n_intervals) return;
+  const IntervalDev iv = a.iv[ivx];
+  __shared__ uint32_t s_first, s_last, s_gap;
+  __shared__ unsigned long long s_lo;
+  if (threadIdx.x == 0) {
+    s_first = kNone;
+    s_last = 0;
+    s_gap = 0;
+    s_lo = ~0ull;
+  }
+  __syncthreads();
+  uint32_t my_first = kNone, my_last = 0, my_gap = 0;
+  for (uint32_t i = threadIdx.x; i < iv.n_tiles; i += blockDim.x) {
+    const TilePartial P = a.partials[iv.tile_begin + i];
+    if (!P.count) continue;
+    my_first = min(my_first, i);
+    my_last = max(my_last, i + 1);
+    my_gap = max(my_gap, max(P.max_gap, P.bgap));
+  }
+  atomicMin(&s_first, my_first);
+  atomicMax(&s_last, my_last);
+  atomicMax(&s_gap, my_gap);
+  __syncthreads();
+  const uint32_t G = s_gap;
+  unsigned long long my_lo = ~0ull;
+  if (G) {
+    for (uint32_t i = threadIdx.x; i < iv.n_tiles; i += blockDim.x) {
+      const TilePartial P = a.partials[iv.tile_begin + i];
+      if (!P.count) continue;
+      const uint64_t vt = 30ull * (iv.k0 + 4ull * a.tile_words * i);
+      if (P.max_gap == G) my_lo = min(my_lo, (unsigned long long)(vt + P.max_lo));
+      if (P.bgap == G) my_lo = min(my_lo, (unsigned long long)P.bgap_lo);
+    }
+  }
+  atomicMin(&s_lo, my_lo);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    IntervalOut o;
+    if (s_first == kNone) {
+      o.first = o.last = 0;
+    } else {
+      const TilePartial F = a.partials[iv.tile_begin + s_first];
+      const TilePartial L = a.partials[iv.tile_begin + s_last - 1];
+      o.first = 30ull * (iv.k0 + 4ull * a.tile_words * s_first) + F.first;
+      o.last = 30ull * (iv.k0 + 4ull * a.tile_words * (s_last - 1)) + L.last;
+    }
+    o.max_gap = G;
+    o.max_gap_lo = G ? s_lo : 0;
+    out[ivx] = o;
+  }
+}
+
+// ---- shared-memory RMW probe ------------------------------------------------------------
+constexpr int kProbeWords = 8192;
+constexpr int kProbeIters = 4096;
+
+__global__ void __launch_bounds__(1024) smem_rmw_probe_kernel(uint32_t* sink) {
+  __shared__ uint32_t s[kProbeWords];
+  for (int i = threadIdx.x; i < kProbeWords; i += blockDim.x) s[i] = 0xFFFFFFFFu;
+  __syncthreads();
+  uint32_t idx = threadIdx.x;
+#pragma unroll 8
+  for (int it = 0; it < kProbeIters; ++it) {
+    atomicAnd(&s[idx & (kProbeWords - 1)], ~(1u << (it & 31)));
+    idx += 1024u;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) sink[blockIdx.x] = s[blockIdx.x & (kProbeWords - 1)];
+}
+
+// ---- host side ------------------------------------------------------------------------------
+static const int kW30h[8] = {1, 7, 11, 13, 17, 19, 23, 29};
+
+static int ensure_tables() {
+  if (g_tables_ready) return 0;
+  uint8_t step[64];
+  int8_t rb[32];
+  for (int r = 0; r < 32; ++r) rb[r] = -1;
+  for (int i = 0; i < 8; ++i) rb[kW30h[i]] = (int8_t)i;
+  for (int bi = 0; bi < 8; ++bi)
+    for (int o = 0; o < 8; ++o) {
+      const int bw = kW30h[bi] * kW30h[o];
+      step[bi * 8 + o] = (uint8_t)((bw / 30) | (rb[bw % 30] << 5));
+    }
+  if (cudaMemcpyToSymbol(c_wheel_step, step, sizeof(step)) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(c_res_bit, rb, sizeof(rb)) != cudaSuccess) return -1;
+  g_tables_ready = true;
+  return 0;
+}
+
+void build_presieve_tables(uint32_t* out) {
+  static const uint32_t groups[kPreGroups][3] = {{7, 11, 13}, {17, 19, 0}, {23, 29, 0}, {31, 0, 0}};
+  for (int g = 0; g < kPreGroups; ++g) {
+    const uint32_t P = kPreMod[g];
+    for (uint32_t j = 0; j < P; ++j) {
+      uint32_t m = 0xFFFFFFFFu;
+      for (uint32_t jb = 0; jb < 4; ++jb)
+        for (uint32_t o = 0; o < 8; ++o) {
+          const uint64_t k = 4ull * j + jb;  // byte index modulo P
+          for (int q = 0; q < 3 && groups[g][q]; ++q) {
+            const uint32_t p = groups[g][q];
+            if ((30ull * k + kW30h[o]) % p == 0) m &= ~(1u << (8 * jb + o));
+          }
+        }
+      out[kPreOff[g] + j] = m;
+    }
+  }
+}
+
+size_t sieve_smem_bytes(uint32_t tile_words) {
+  return (size_t)(tile_words + kPreWords + kSmCounters) * sizeof(uint32_t);
+}
+
+template <int BLOCK, bool EMIT>
+static int set_attrs(size_t smem) {
+  auto fn = sieve_tiles_kernel<BLOCK, EMIT>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return -1;
+  return 0;
+}
+
+int sieve_kernel_attrs(int block, size_t smem, int* max_ctas_per_sm) {
+  if (ensure_tables()) return -1;
+  int rc = 0, n = 0;
+  if (block == 512) {
+    rc |= set_attrs<512, false>(smem) | set_attrs<512, true>(smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sieve_tiles_kernel<512, false>, 512, smem) != cudaSuccess) rc = -1;
+  } else if (block == 1024) {
+    rc |= set_attrs<1024, false>(smem) | set_attrs<1024, true>(smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sieve_tiles_kernel<1024, false>, 1024, smem) != cudaSuccess) rc = -1;
+  } else {
+    return -1;
+  }
+  if (max_ctas_per_sm) *max_ctas_per_sm = n;
+  return rc;
+}
+
+int launch_sieve_stats(const SieveArgs& a, int grid, int block, size_t smem, void* stream) {
+  if (ensure_tables()) return -1;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (block == 512) sieve_tiles_kernel<512, false><<<grid, 512, smem, s>>>(a);
+  else if (block == 1024) sieve_tiles_kernel<1024, false><<<grid, 1024, smem, s>>>(a);
+  else return -1;
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_sieve_emit(const SieveArgs& a, int grid, int block, size_t smem, void* stream) {
+  if (ensure_tables()) return -1;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (block == 512) sieve_tiles_kernel<512, true><<<grid, 512, smem, s>>>(a);
+  else if (block == 1024) sieve_tiles_kernel<1024, true><<<grid, 1024, smem, s>>>(a);
+  else return -1;
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_stitch(const SieveArgs& a, void* stream) {
+  if (a.n_tiles == 0) return 0;
+  const int blk = 256;
+  stitch_kernel<<<(a.n_tiles + blk - 1) / blk, blk, 0, (cudaStream_t)stream>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_reduce(const SieveArgs& a, IntervalOut* out, void* stream) {
+  if (a.n_intervals == 0) return 0;
+  reduce_kernel<<<a.n_intervals, 256, 0, (cudaStream_t)stream>>>(a, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int probe_smem_rmw(int sm_count, void* stream, float* ms, double* bytes) {
+  cudaStream_t s = (cudaStream_t)stream;
+  const int grid = sm_count * 2;
+  uint32_t* sink = nullptr;
+  if (cudaMalloc(&sink, grid * sizeof(uint32_t)) != cudaSuccess) return -1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  smem_rmw_probe_kernel<<<grid, 1024, 0, s>>>(sink);  // warm-up
+  cudaEventRecord(e0, s);
+  const int reps = 5;
+  for (int r = 0; r < reps; ++r) smem_rmw_probe_kernel<<<grid, 1024, 0, s>>>(sink);
+  cudaEventRecord(e1, s);
+  cudaError_t st = cudaEventSynchronize(e1);
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  if (st != cudaSuccess) return -1;
+  *ms = t / reps;
+  *bytes = (double)grid * 1024.0 * kProbeIters * 8.0;
+  return 0;
+}
+
+}  // namespace voss

@@ -1,0 +1,787 @@
+// voss_api.cpp — host runtime and C ABI of libvoss.so (declared in include/voss.h).
+//
+// Replaces the host half of src/voss_v7_live.cu main() (:337-837): base-prime generation
+// (:96-118), the segment loop's launch-list building and host accumulation (:434-626), the
+// epilogue statistics (:634-705) and the CSV writers (:707-827); and the driver half of
+// src/verify_cpp.cpp main() (:112-276) for batch Miller-Rabin and gap proofs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <cinttypes>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "voss.h"
+#include "voss_internal.h"
+
+using namespace voss;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CUDA_TRY(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e__ = (call);                                                            \
+    if (e__ != cudaSuccess)                                                              \
+      return fail(VOSS_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e__));      \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  int ensure(size_t need) {
+    if (need <= bytes) return VOSS_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t n = need < 256 ? 256 : need + need / 4;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return fail(VOSS_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", n, cudaGetErrorString(e));
+    }
+    bytes = n;
+    return VOSS_OK;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+const int kW30[8] = {1, 7, 11, 13, 17, 19, 23, 29};
+const int kQ[VOSS_NUM_Q] = VOSS_Q_LIST;
+constexpr uint64_t kMaxHi = 1ull << 62;
+constexpr uint32_t kOverCap = 1u << 16;
+constexpr uint64_t kDefaultLargeCap = 1ull << 22;
+constexpr uint64_t kMaxLargeCap = 50000000ull;  // MAX_LARGE_GAPS, src/voss_v7_live.cu:34
+
+uint64_t isqrt_u64(uint64_t x) {
+  uint64_t s = (uint64_t)std::sqrt((long double)x);
+  while (s * s > x) --s;
+  while ((s + 1) * (s + 1) <= x) ++s;
+  return s;
+}
+
+// Primes 37 <= p <= limit, by an odd-only segmented sieve.
+std::vector<uint32_t> base_primes(uint64_t limit) {
+  std::vector<uint32_t> out;
+  if (limit < 37) return out;
+  const uint64_t r = isqrt_u64(limit);
+  std::vector<uint8_t> small(r + 1, 1);
+  std::vector<uint32_t> sp;
+  for (uint64_t i = 2; i <= r; ++i) {
+    if (!small[i]) continue;
+    sp.push_back((uint32_t)i);
+    for (uint64_t j = i * i; j <= r; j += i) small[j] = 0;
+  }
+  out.reserve((size_t)(limit / (std::log((double)limit) - 1.1)) + 16);
+  const uint64_t SEG = 1u << 21;  // odd slots per segment
+  std::vector<uint8_t> seg(SEG);
+  for (uint64_t base = 0; base <= limit; base += 2 * SEG) {
+    // slot i <-> value base + 2i + 1
+    std::fill(seg.begin(), seg.end(), 1);
+    const uint64_t vmax = std::min(limit, base + 2 * SEG - 1);
+    for (uint32_t q : sp) {
+      if (q == 2) continue;
+      const uint64_t qq = (uint64_t)q * q;
+      if (qq > vmax) break;
+      uint64_t m = std::max(qq, (base + 1 + q - 1) / q * q);
+      if ((m & 1) == 0) m += q;
+      for (uint64_t i = (m - base - 1) / 2; i < SEG; i += q) seg[i] = 0;
+    }
+    for (uint64_t i = 0; i < SEG; ++i) {
+      const uint64_t v = base + 2 * i + 1;
+      if (v > vmax) break;
+      if (seg[i] && v >= 37) out.push_back((uint32_t)v);
+    }
+  }
+  return out;
+}
+
+struct Workspace {
+  DevBuf iv, partials, acc, out, large, large_iv, over, counters, istats, offsets, emit, mr_work;
+};
+
+}  // namespace
+
+namespace voss_detail {
+int set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace voss_detail
+
+struct voss_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  uint64_t max_hi = 0;
+  std::vector<uint32_t> primes;  // >= 37
+  DevBuf d_primes, d_magic, d_pretab;
+  voss_tuning tune{};
+  int ctas_per_sm = 1;
+  Workspace ws;
+  // last range run
+  bool have_range = false;
+  uint64_t r_lo = 0, r_hi = 0, r_seg = 0;
+  uint32_t r_flags = 0;
+  uint32_t r_tiles = 0;
+  uint64_t r_large_cap = 0;
+  float sieve_ms = 0, total_ms = 0;
+};
+
+namespace {
+
+int apply_tuning(voss_ctx* c, const voss_tuning& t0) {
+  voss_tuning t = t0;
+  if (!t.block_threads) t.block_threads = 1024;
+  if (!t.chunk_words) t.chunk_words = t.block_threads == 1024 ? 49 : 45;
+  if (!t.coop_div) t.coop_div = 32;
+  if (!t.mult_factor) t.mult_factor = 8;
+  if (t.block_threads != 512 && t.block_threads != 1024)
+    return fail(VOSS_ERR_ARG, "block_threads must be 512 or 1024");
+  if ((t.chunk_words & 1u) == 0 || t.chunk_words > 255)
+    return fail(VOSS_ERR_ARG, "chunk_words must be odd and <= 255");
+  const uint32_t tw = t.block_threads * t.chunk_words;
+  const size_t smem = sieve_smem_bytes(tw);
+  int maxc = 0;
+  cudaSetDevice(c->device);
+  if (sieve_kernel_attrs((int)t.block_threads, smem, &maxc) != 0 || maxc < 1)
+    return fail(VOSS_ERR_ARG, "tile of %u words does not fit in shared memory (%zu bytes)", tw, smem);
+  if (!t.ctas_per_sm || (int)t.ctas_per_sm > maxc) t.ctas_per_sm = (uint32_t)maxc;
+  c->tune = t;
+  c->ctas_per_sm = (int)t.ctas_per_sm;
+  return VOSS_OK;
+}
+
+struct RunPlan {
+  std::vector<IntervalDev> iv;
+  uint32_t n_tiles = 0;
+};
+
+// Cut intervals [lo_i, hi_i) into tiles; intervals without wheel integers get no tiles.
+int plan_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, uint32_t n,
+                   uint64_t seg_k, RunPlan* P) {
+  const uint64_t tw = (uint64_t)c->tune.block_threads * c->tune.chunk_words;
+  P->iv.resize(n);
+  uint64_t tiles = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    IntervalDev& d = P->iv[i];
+    std::memset(&d, 0, sizeof(d));
+    const uint64_t a = std::max<uint64_t>(lo[i], 7);
+    d.lo = a;
+    d.hi = hi[i];
+    d.seg_k = seg_k;
+    d.tile_begin = (uint32_t)tiles;
+    if (a >= hi[i]) {
+      d.k0 = 0;
+      d.n_words = 0;
+      d.n_tiles = 0;
+      continue;
+    }
+    const uint64_t kf = a / 30, kl = (hi[i] - 1) / 30;
+    d.k0 = kf & ~3ull;
+    d.n_words = (kl - d.k0) / 4 + 1;
+    const uint64_t nt = (d.n_words + tw - 1) / tw;
+    d.n_tiles = (uint32_t)nt;
+    tiles += nt;
+    if (tiles >= 0x7FFFFFFFull) return fail(VOSS_ERR_RANGE, "too many tiles in one launch; split the range");
+  }
+  P->n_tiles = (uint32_t)tiles;
+  return VOSS_OK;
+}
+
+enum { kCtrTile = 0, kCtrLarge = 1, kCtrOver = 2, kCtrError = 3, kCtrMrWork = 4, kCtrWords = 8 };
+
+int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_cap, bool emit,
+                cudaStream_t s) {
+  Workspace& W = c->ws;
+  const uint32_t n_iv = (uint32_t)P.iv.size();
+  int rc;
+  if ((rc = W.iv.ensure(sizeof(IntervalDev) * std::max<size_t>(1, n_iv)))) return rc;
+  if ((rc = W.partials.ensure(sizeof(TilePartial) * std::max<size_t>(1, P.n_tiles)))) return rc;
+  if ((rc = W.acc.ensure(sizeof(unsigned long long) * kAccStride * std::max<size_t>(1, n_iv)))) return rc;
+  if ((rc = W.out.ensure(sizeof(IntervalOut) * std::max<size_t>(1, n_iv)))) return rc;
+  if ((rc = W.counters.ensure(sizeof(uint32_t) * kCtrWords))) return rc;
+  if ((rc = W.over.ensure(sizeof(OverflowGap) * kOverCap))) return rc;
+  const uint64_t cap = want_large ? std::min(std::max(large_cap, (uint64_t)1), kMaxLargeCap) : 1;
+  if ((rc = W.large.ensure(sizeof(LargeGapDev) * cap))) return rc;
+  if ((rc = W.large_iv.ensure(sizeof(uint32_t) * cap))) return rc;
+  if (n_iv) CUDA_TRY(cudaMemcpyAsync(W.iv.p, P.iv.data(), sizeof(IntervalDev) * n_iv, cudaMemcpyHostToDevice, s));
+  if (!emit) CUDA_TRY(cudaMemsetAsync(W.acc.p, 0, sizeof(unsigned long long) * kAccStride * std::max<size_t>(1, n_iv), s));
+  CUDA_TRY(cudaMemsetAsync(W.counters.p, 0, sizeof(uint32_t) * kCtrWords, s));
+
+  SieveArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.primes = c->d_primes.as<uint32_t>();
+  a.magic = c->d_magic.as<uint64_t>();
+  a.n_primes = (uint32_t)c->primes.size();
+  a.pretab = c->d_pretab.as<uint32_t>();
+  a.iv = W.iv.as<IntervalDev>();
+  a.n_intervals = n_iv;
+  a.n_tiles = P.n_tiles;
+  a.tile_words = c->tune.block_threads * c->tune.chunk_words;
+  a.chunk_words = c->tune.chunk_words;
+  a.coop_div = c->tune.coop_div;
+  a.mult_factor = c->tune.mult_factor;
+  a.want_large = want_large ? 1u : 0u;
+  uint32_t* ctr = W.counters.as<uint32_t>();
+  a.tile_counter = ctr + kCtrTile;
+  a.large_count = ctr + kCtrLarge;
+  a.over_count = ctr + kCtrOver;
+  a.error = ctr + kCtrError;
+  a.partials = W.partials.as<TilePartial>();
+  a.acc = W.acc.as<unsigned long long>();
+  a.large = W.large.as<LargeGapDev>();
+  a.large_iv = W.large_iv.as<uint32_t>();
+  a.large_cap = (uint32_t)cap;
+  a.over = W.over.as<OverflowGap>();
+  a.over_cap = kOverCap;
+  if (emit) {
+    a.tile_offset = W.offsets.as<unsigned long long>();
+    a.out = W.emit.as<unsigned long long>();
+    a.out_cap = W.emit.bytes / sizeof(unsigned long long);
+  }
+  const uint32_t tw = a.tile_words;
+  const size_t smem = sieve_smem_bytes(tw);
+  const int slots = c->sm_count * c->ctas_per_sm;
+  const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(P.n_tiles, (uint32_t)slots));
+  CUDA_TRY(cudaEventRecord(c->ev0, s));
+  if (P.n_tiles) {
+    int lr = emit ? launch_sieve_emit(a, grid, (int)c->tune.block_threads, smem, s)
+                  : launch_sieve_stats(a, grid, (int)c->tune.block_threads, smem, s);
+    if (lr) return fail(VOSS_ERR_CUDA, "sieve launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  CUDA_TRY(cudaEventRecord(c->ev1, s));
+  if (!emit) {
+    if (launch_stitch(a, s)) return fail(VOSS_ERR_CUDA, "stitch launch failed");
+    if (launch_reduce(a, W.out.as<IntervalOut>(), s)) return fail(VOSS_ERR_CUDA, "reduce launch failed");
+  }
+  CUDA_TRY(cudaEventRecord(c->ev2, s));
+  return VOSS_OK;
+}
+
+int check_device_error(voss_ctx* c, uint32_t* ctr_host) {
+  if (ctr_host[kCtrError] & kErrBounds) return fail(VOSS_ERR_DEVICE, "kernel bounds check failed");
+  if (ctr_host[kCtrError] & kErrOverflowList) return fail(VOSS_ERR_DEVICE, "gap overflow list full");
+  if (ctr_host[kCtrError]) return fail(VOSS_ERR_DEVICE, "kernel error word 0x%x", ctr_host[kCtrError]);
+  (void)c;
+  return VOSS_OK;
+}
+
+// Small primes 2, 3, 5 are outside the wheel; return those in [lo, hi).
+std::vector<uint64_t> small_primes_in(uint64_t lo, uint64_t hi) {
+  std::vector<uint64_t> v;
+  for (uint64_t p : {2ull, 3ull, 5ull})
+    if (p >= lo && p < hi) v.push_back(p);
+  return v;
+}
+
+int row30(uint64_t p) {
+  const int r = (int)(p % 30);
+  for (int i = 0; i < 8; ++i)
+    if (kW30[i] == r) return i;
+  return -1;
+}
+
+// Fold the device accumulators of one range into voss_range_stats (without large gaps).
+void finalize_range(const unsigned long long* acc, const IntervalOut& o, uint64_t lo, uint64_t hi,
+                    uint32_t flags, uint64_t seg_num, const std::vector<OverflowGap>& over,
+                    voss_range_stats* st) {
+  const bool compat = (flags & VOSS_FLAG_REF_COMPAT) != 0;
+  std::memset(st, 0, sizeof(*st));
+  st->lo = lo;
+  st->hi = hi;
+  st->flags = flags;
+  st->seg_num = compat ? seg_num : 0;
+  st->prime_count = acc[kAccCount];
+  // gap histogram: bins g/2; for g < 100 add the per-residue bins
+  for (int b = 1; b < kHistBins; ++b) {
+    uint64_t v = acc[kAccHist + b];
+    if (b < kModqBins)
+      for (int r = 0; r < 8; ++r) v += acc[kAccModq + r * kModqBins + b];
+    if (2 * b < VOSS_MAX_GAP) st->gap_hist[2 * b] += v;
+  }
+  for (const OverflowGap& g : over)
+    if (g.gap < VOSS_MAX_GAP) st->gap_hist[g.gap]++;
+  // per-residue gap histogram rows (q = 6 rows {1,5}, then q = 30 rows W30)
+  for (int r = 0; r < 8; ++r) {
+    const int row6 = (kW30[r] % 6 == 1) ? 0 : 1;
+    for (int b = 1; b < kModqBins; ++b) {
+      const uint64_t v = acc[kAccModq + r * kModqBins + b];
+      st->modq_gap[row6][2 * b] += v;
+      st->modq_gap[2 + r][2 * b] += v;
+    }
+  }
+  // residue classes -> mod 4 and mod q (840 = 0 mod 3,4,5,6,7,8,12,30; 4290 = 0 mod 11,13)
+  int off[VOSS_NUM_Q];
+  for (int qi = 0, s = 0; qi < VOSS_NUM_Q; ++qi) {
+    off[qi] = s;
+    s += kQ[qi];
+  }
+  for (int c = 0; c < 28; ++c)
+    for (int r = 0; r < 8; ++r) {
+      const uint64_t n = acc[kAccCls28 + c * 8 + r];
+      if (!n) continue;
+      const uint64_t v = 30ull * c + kW30[r];
+      if ((v & 3) == 1) st->mod4[0] += n;
+      else if ((v & 3) == 3) st->mod4[1] += n;
+      for (int qi = 0; qi < VOSS_NUM_Q; ++qi) {
+        const int q = kQ[qi];
+        if (q == 11 || q == 13) continue;
+        st->modq[off[qi] + (int)(v % q)] += n;
+      }
+    }
+  for (int c = 0; c < 143; ++c)
+    for (int r = 0; r < 8; ++r) {
+      const uint64_t n = acc[kAccCls143 + c * 8 + r];
+      if (!n) continue;
+      const uint64_t v = 30ull * c + kW30[r];
+      st->modq[off[6] + (int)(v % 11)] += n;
+      st->modq[off[8] + (int)(v % 13)] += n;
+    }
+  st->first_prime = o.first;
+  st->last_prime = o.last;
+  st->max_gap = o.max_gap;
+  st->max_gap_lo = o.max_gap_lo;
+
+  // primes 2, 3, 5 and their gaps (they come first in the order of primes)
+  const std::vector<uint64_t> sp = small_primes_in(lo, hi);
+  if (!sp.empty()) {
+    std::vector<uint64_t> seq = sp;
+    if (o.first) seq.push_back(o.first);
+    uint64_t sm_max = 0, sm_lo = 0;
+    for (size_t i = 1; i < seq.size(); ++i) {
+      const uint64_t g = seq[i] - seq[i - 1];
+      if (g < VOSS_MAX_GAP) st->gap_hist[g]++;
+      if (g > sm_max) {
+        sm_max = g;
+        sm_lo = seq[i - 1];
+      }
+    }
+    if (sm_max >= st->max_gap) {  // earlier pairs win ties
+      st->max_gap = sm_max;
+      st->max_gap_lo = sm_lo;
+    }
+    st->prime_count += sp.size();
+    st->first_prime = sp.front();
+    if (!o.last) st->last_prime = sp.back();
+    for (uint64_t p : sp) {
+      if ((p & 3) == 1) st->mod4[0]++;
+      else if ((p & 3) == 3) st->mod4[1]++;
+      if (!compat)
+        for (int qi = 0; qi < VOSS_NUM_Q; ++qi) st->modq[off[qi] + (int)(p % kQ[qi])]++;
+    }
+  }
+}
+
+int fetch_common(voss_ctx* c, uint32_t n_iv, std::vector<unsigned long long>& acc,
+                 std::vector<IntervalOut>& outs, uint32_t* ctr, std::vector<OverflowGap>& over,
+                 bool want_acc) {
+  cudaStream_t s = c->stream;
+  CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(uint32_t) * kCtrWords, cudaMemcpyDeviceToHost, s));
+  outs.resize(std::max<uint32_t>(1, n_iv));
+  CUDA_TRY(cudaMemcpyAsync(outs.data(), c->ws.out.p, sizeof(IntervalOut) * n_iv, cudaMemcpyDeviceToHost, s));
+  if (want_acc) {
+    acc.resize((size_t)kAccStride * std::max<uint32_t>(1, n_iv));
+    CUDA_TRY(cudaMemcpyAsync(acc.data(), c->ws.acc.p, sizeof(unsigned long long) * kAccStride * n_iv,
+                             cudaMemcpyDeviceToHost, s));
+  }
+  CUDA_TRY(cudaStreamSynchronize(s));
+  int rc = check_device_error(c, ctr);
+  if (rc) return rc;
+  const uint32_t no = std::min(ctr[kCtrOver], kOverCap);
+  over.resize(no);
+  if (no) CUDA_TRY(cudaMemcpy(over.data(), c->ws.over.p, sizeof(OverflowGap) * no, cudaMemcpyDeviceToHost));
+  return VOSS_OK;
+}
+
+int run_range_device(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t flags, uint64_t seg_num,
+                     uint64_t large_cap, cudaStream_t s) {
+  const bool compat = (flags & VOSS_FLAG_REF_COMPAT) != 0;
+  if (hi < lo) return fail(VOSS_ERR_ARG, "hi < lo");
+  if (hi > c->max_hi) return fail(VOSS_ERR_RANGE, "hi = %" PRIu64 " exceeds the context limit %" PRIu64, hi, c->max_hi);
+  uint64_t seg_k = 0;
+  if (compat) {
+    if (seg_num == 0 || seg_num % 30) return fail(VOSS_ERR_ARG, "seg_num must be a positive multiple of 30");
+    seg_k = seg_num / 30;
+    const uint64_t tile_bytes = 4ull * c->tune.block_threads * c->tune.chunk_words;
+    if (seg_k < tile_bytes)
+      return fail(VOSS_ERR_ARG, "seg_num/30 = %" PRIu64 " is below the tile size %" PRIu64 " bytes", seg_k, tile_bytes);
+  }
+  RunPlan P;
+  int rc = plan_intervals(c, &lo, &hi, 1, seg_k, &P);
+  if (rc) return rc;
+  rc = launch_plan(c, P, true, large_cap, false, s);
+  if (rc) return rc;
+  c->have_range = true;
+  c->r_lo = lo;
+  c->r_hi = hi;
+  c->r_seg = compat ? seg_num : 0;
+  c->r_flags = flags;
+  c->r_tiles = P.n_tiles;
+  c->r_large_cap = std::min(std::max(large_cap, (uint64_t)1), kMaxLargeCap);
+  return VOSS_OK;
+}
+
+int fetch_range(voss_ctx* c, voss_range_stats* st, voss_large_gap* large, uint64_t large_cap,
+                uint64_t* written) {
+  if (!c->have_range) return fail(VOSS_ERR_STATE, "no range has been sieved on this context");
+  std::vector<unsigned long long> acc;
+  std::vector<IntervalOut> outs;
+  std::vector<OverflowGap> over;
+  uint32_t ctr[kCtrWords];
+  int rc = fetch_common(c, 1, acc, outs, ctr, over, true);
+  if (rc) return rc;
+  cudaEventElapsedTime(&c->sieve_ms, c->ev0, c->ev1);
+  cudaEventElapsedTime(&c->total_ms, c->ev0, c->ev2);
+  finalize_range(acc.data(), outs[0], c->r_lo, c->r_hi, c->r_flags, c->r_seg, over, st);
+  const uint64_t found = ctr[kCtrLarge];
+  st->large_total = found;
+  const uint64_t ondev = std::min<uint64_t>(found, c->r_large_cap);
+  std::vector<voss_large_gap> lg(ondev);
+  if (ondev)
+    CUDA_TRY(cudaMemcpy(lg.data(), c->ws.large.p, sizeof(voss_large_gap) * ondev, cudaMemcpyDeviceToHost));
+  std::sort(lg.begin(), lg.end(), [](const voss_large_gap& x, const voss_large_gap& y) {
+    return x.position < y.position;
+  });
+  const uint64_t w = std::min<uint64_t>(ondev, large ? large_cap : 0);
+  if (w) std::memcpy(large, lg.data(), sizeof(voss_large_gap) * w);
+  if (written) *written = w;
+  return VOSS_OK;
+}
+
+}  // namespace
+
+// =====================================================================================
+// C ABI
+// =====================================================================================
+extern "C" {
+
+VOSS_API const char* voss_version(void) { return "voss-b200 0.1 (sm_100a)"; }
+
+VOSS_API const char* voss_last_error(void) { return g_err.c_str(); }
+
+VOSS_API int voss_device_count(int* count) {
+  if (!count) return fail(VOSS_ERR_ARG, "count is NULL");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) n = 0;
+  *count = n;
+  return VOSS_OK;
+}
+
+VOSS_API int voss_ctx_create(int device, uint64_t max_hi, voss_ctx** out) {
+  if (!out) return fail(VOSS_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (max_hi < 8 || max_hi > kMaxHi) return fail(VOSS_ERR_ARG, "max_hi must be in [8, 2^62]");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(VOSS_ERR_NODEV, "no CUDA device");
+  if (device < 0 || device >= n) return fail(VOSS_ERR_ARG, "device %d out of range", device);
+  voss_ctx* c = new voss_ctx();
+  c->device = device;
+  c->max_hi = max_hi;
+  auto bail = [&](int code) {
+    voss_ctx_destroy(c);
+    return code;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) return bail(fail(VOSS_ERR_CUDA, "cudaSetDevice failed"));
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return bail(fail(VOSS_ERR_CUDA, "cudaGetDeviceProperties failed"));
+  c->sm_count = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaEventCreate(&c->ev2) != cudaSuccess)
+    return bail(fail(VOSS_ERR_CUDA, "stream/event creation failed"));
+  c->primes = base_primes(isqrt_u64(max_hi - 1));
+  const size_t np = std::max<size_t>(1, c->primes.size());
+  int rc;
+  if ((rc = c->d_primes.ensure(np * sizeof(uint32_t))) || (rc = c->d_magic.ensure(np * sizeof(uint64_t))) ||
+      (rc = c->d_pretab.ensure(kPreWords * sizeof(uint32_t))))
+    return bail(rc);
+  std::vector<uint64_t> magic(np, 0);
+  for (size_t i = 0; i < c->primes.size(); ++i) magic[i] = ~0ull / c->primes[i];
+  std::vector<uint32_t> pre(kPreWords);
+  build_presieve_tables(pre.data());
+  if (!c->primes.empty()) {
+    if (cudaMemcpy(c->d_primes.p, c->primes.data(), c->primes.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->d_magic.p, magic.data(), c->primes.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(fail(VOSS_ERR_CUDA, "base prime upload failed"));
+  }
+  if (cudaMemcpy(c->d_pretab.p, pre.data(), kPreWords * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(fail(VOSS_ERR_CUDA, "presieve table upload failed"));
+  voss_tuning t{};
+  if ((rc = apply_tuning(c, t))) return bail(rc);
+  *out = c;
+  return VOSS_OK;
+}
+
+VOSS_API void voss_ctx_destroy(voss_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev2) cudaEventDestroy(c->ev2);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+VOSS_API int voss_ctx_info(const voss_ctx* c, uint64_t* max_hi, uint64_t* n_base_primes, int* sm_count) {
+  if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
+  if (max_hi) *max_hi = c->max_hi;
+  if (n_base_primes) {
+    // base primes >= 7 up to isqrt(max_hi - 1): the table (>= 37) plus 7..31 when in range
+    const uint64_t lim = isqrt_u64(c->max_hi - 1);
+    uint64_t small = 0;
+    for (uint64_t p : {7ull, 11ull, 13ull, 17ull, 19ull, 23ull, 29ull, 31ull})
+      if (p <= lim) ++small;
+    *n_base_primes = c->primes.size() + small;
+  }
+  if (sm_count) *sm_count = c->sm_count;
+  return VOSS_OK;
+}
+
+VOSS_API int voss_ctx_set_tuning(voss_ctx* c, const voss_tuning* t) {
+  if (!c || !t) return fail(VOSS_ERR_ARG, "NULL argument");
+  return apply_tuning(c, *t);
+}
+
+VOSS_API int voss_ctx_get_tuning(const voss_ctx* c, voss_tuning* t) {
+  if (!c || !t) return fail(VOSS_ERR_ARG, "NULL argument");
+  *t = c->tune;
+  return VOSS_OK;
+}
+
+VOSS_API int voss_sieve_range_device(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t flags,
+                                     uint64_t seg_num, void* stream) {
+  if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  int rc = run_range_device(c, lo, hi, flags, seg_num, kDefaultLargeCap, s);
+  if (rc) return rc;
+  if (s != c->stream) {  // later fetches run on the context stream
+    cudaEvent_t e;
+    CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(e, s));
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, e, 0));
+    cudaEventDestroy(e);
+  }
+  return VOSS_OK;
+}
+
+VOSS_API int voss_fetch_range(voss_ctx* c, voss_range_stats* st, voss_large_gap* large,
+                              uint64_t large_cap, uint64_t* written) {
+  if (!c || !st) return fail(VOSS_ERR_ARG, "NULL argument");
+  cudaSetDevice(c->device);
+  return fetch_range(c, st, large, large_cap, written);
+}
+
+VOSS_API int voss_sieve_range(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t flags, uint64_t seg_num,
+                              voss_range_stats* st, voss_large_gap* large, uint64_t large_cap,
+                              uint64_t* written) {
+  if (!c || !st) return fail(VOSS_ERR_ARG, "NULL argument");
+  cudaSetDevice(c->device);
+  int rc = run_range_device(c, lo, hi, flags, seg_num, std::max(large_cap, kDefaultLargeCap), c->stream);
+  if (rc) return rc;
+  return fetch_range(c, st, large, large_cap, written);
+}
+
+VOSS_API int voss_last_kernel_ms(const voss_ctx* c, double* sieve_ms, double* total_ms) {
+  if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
+  if (sieve_ms) *sieve_ms = c->sieve_ms;
+  if (total_ms) *total_ms = c->total_ms;
+  return VOSS_OK;
+}
+
+VOSS_API int voss_sieve_intervals(voss_ctx* c, const uint64_t* lo, const uint64_t* hi, uint32_t n,
+                                  voss_interval_stats* out) {
+  if (!c || (n && (!lo || !hi || !out))) return fail(VOSS_ERR_ARG, "NULL argument");
+  cudaSetDevice(c->device);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (hi[i] < lo[i]) return fail(VOSS_ERR_ARG, "interval %u has hi < lo", i);
+    if (hi[i] > c->max_hi) return fail(VOSS_ERR_RANGE, "interval %u exceeds the context limit", i);
+  }
+  if (n == 0) return VOSS_OK;
+  RunPlan P;
+  int rc = plan_intervals(c, lo, hi, n, 0, &P);
+  if (rc) return rc;
+  rc = launch_plan(c, P, false, 0, false, c->stream);
+  if (rc) return rc;
+  std::vector<unsigned long long> acc;
+  std::vector<IntervalOut> outs;
+  std::vector<OverflowGap> over;
+  uint32_t ctr[kCtrWords];
+  rc = fetch_common(c, n, acc, outs, ctr, over, true);
+  if (rc) return rc;
+  cudaEventElapsedTime(&c->sieve_ms, c->ev0, c->ev1);
+  cudaEventElapsedTime(&c->total_ms, c->ev0, c->ev2);
+  for (uint32_t i = 0; i < n; ++i) {
+    const unsigned long long* A = acc.data() + (size_t)i * kAccStride;
+    voss_interval_stats& s = out[i];
+    std::memset(&s, 0, sizeof(s));
+    s.lo = lo[i];
+    s.hi = hi[i];
+    s.prime_count = A[kAccCount];
+    for (int b = 1; b < kHistBins; ++b) {
+      uint64_t v = A[kAccHist + b];
+      if (b < kModqBins)
+        for (int r = 0; r < 8; ++r) v += A[kAccModq + r * kModqBins + b];
+      s.gap_hist[b] = v;
+    }
+    s.gap_overflow = A[kAccHistOver];
+    s.first_prime = outs[i].first;
+    s.last_prime = outs[i].last;
+    s.max_gap = outs[i].max_gap;
+    s.max_gap_lo = outs[i].max_gap_lo;
+    const std::vector<uint64_t> sp = small_primes_in(lo[i], hi[i]);
+    if (!sp.empty()) {
+      std::vector<uint64_t> seq = sp;
+      if (outs[i].first) seq.push_back(outs[i].first);
+      uint64_t sm_max = 0, sm_lo = 0;
+      for (size_t k = 1; k < seq.size(); ++k) {
+        const uint64_t g = seq[k] - seq[k - 1];
+        s.gap_hist[g >> 1]++;
+        if (g > sm_max) {
+          sm_max = g;
+          sm_lo = seq[k - 1];
+        }
+      }
+      if (sm_max >= s.max_gap) {
+        s.max_gap = sm_max;
+        s.max_gap_lo = sm_lo;
+      }
+      s.prime_count += sp.size();
+      s.first_prime = sp.front();
+      if (!outs[i].last) s.last_prime = sp.back();
+    }
+  }
+  return VOSS_OK;
+}
+
+VOSS_API int voss_primes_range(voss_ctx* c, uint64_t lo, uint64_t hi, uint64_t* out, uint64_t cap,
+                               uint64_t* count) {
+  if (!c || !count || (cap && !out)) return fail(VOSS_ERR_ARG, "NULL argument");
+  if (hi < lo) return fail(VOSS_ERR_ARG, "hi < lo");
+  if (hi > c->max_hi) return fail(VOSS_ERR_RANGE, "hi exceeds the context limit");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  RunPlan P;
+  int rc = plan_intervals(c, &lo, &hi, 1, 0, &P);
+  if (rc) return rc;
+  // pass 1: per-tile counts
+  rc = launch_plan(c, P, false, 0, false, s);
+  if (rc) return rc;
+  std::vector<TilePartial> parts(P.n_tiles);
+  if (P.n_tiles)
+    CUDA_TRY(cudaMemcpyAsync(parts.data(), c->ws.partials.p, sizeof(TilePartial) * P.n_tiles, cudaMemcpyDeviceToHost, s));
+  uint32_t ctr[kCtrWords];
+  CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if ((rc = check_device_error(c, ctr))) return rc;
+  std::vector<unsigned long long> offs(std::max<uint32_t>(1, P.n_tiles));
+  uint64_t total = 0;
+  for (uint32_t t = 0; t < P.n_tiles; ++t) {
+    offs[t] = total;
+    total += parts[t].count;
+  }
+  const std::vector<uint64_t> sp = small_primes_in(lo, hi);
+  *count = total + sp.size();
+  uint64_t k = 0;
+  for (uint64_t p : sp) {
+    if (k < cap) out[k] = p;
+    ++k;
+  }
+  if (total == 0 || k >= cap) return VOSS_OK;
+  const uint64_t room = std::min<uint64_t>(total, cap - k);
+  if ((rc = c->ws.offsets.ensure(sizeof(unsigned long long) * offs.size()))) return rc;
+  if ((rc = c->ws.emit.ensure(sizeof(unsigned long long) * room))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(c->ws.offsets.p, offs.data(), sizeof(unsigned long long) * P.n_tiles, cudaMemcpyHostToDevice, s));
+  // pass 2: write (out_cap is the buffer size, which may exceed `room`)
+  rc = launch_plan(c, P, false, 0, true, s);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(out + k, c->ws.emit.p, sizeof(uint64_t) * room, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return check_device_error(c, ctr);
+}
+
+VOSS_API int voss_mr_verify_device(voss_ctx* c, const uint64_t* d_n, uint64_t count, uint8_t* d_out,
+                                   void* stream) {
+  if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
+  if (count && (!d_n || !d_out)) return fail(VOSS_ERR_ARG, "NULL argument");
+  if (count > 0xFFFFFFFFull) return fail(VOSS_ERR_ARG, "count must be < 2^32 per call");
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  int rc;
+  if ((rc = c->ws.mr_work.ensure(sizeof(uint32_t) * (std::max<uint64_t>(count, 1) + 8)))) return rc;
+  uint32_t* work = c->ws.mr_work.as<uint32_t>();
+  if (launch_mr(d_n, count, d_out, work + 8, work, s, c->sm_count))
+    return fail(VOSS_ERR_CUDA, "Miller-Rabin launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return VOSS_OK;
+}
+
+VOSS_API int voss_mr_verify(voss_ctx* c, const uint64_t* n, uint64_t count, uint8_t* is_prime) {
+  if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
+  if (count == 0) return VOSS_OK;
+  if (!n || !is_prime) return fail(VOSS_ERR_ARG, "NULL argument");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  DevBuf dn, dout;
+  int rc;
+  if ((rc = dn.ensure(count * 8)) || (rc = dout.ensure(count))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(dn.p, n, count * 8, cudaMemcpyHostToDevice, s));
+  if ((rc = voss_mr_verify_device(c, dn.as<uint64_t>(), count, dout.as<uint8_t>(), s))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(is_prime, dout.p, count, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return VOSS_OK;
+}
+
+VOSS_API int voss_prove_gaps(voss_ctx* c, const uint64_t* p_after, const int32_t* gap, uint64_t count,
+                             uint8_t* ok) {
+  if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
+  if (count == 0) return VOSS_OK;
+  if (!p_after || !gap || !ok) return fail(VOSS_ERR_ARG, "NULL argument");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  DevBuf dp, dg, dok;
+  int rc;
+  if ((rc = dp.ensure(count * 8)) || (rc = dg.ensure(count * 4)) || (rc = dok.ensure(count))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(dp.p, p_after, count * 8, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(dg.p, gap, count * 4, cudaMemcpyHostToDevice, s));
+  if (launch_prove_gaps(dp.as<uint64_t>(), dg.as<int32_t>(), count, dok.as<uint8_t>(), s, c->sm_count))
+    return fail(VOSS_ERR_CUDA, "gap proof launch failed");
+  CUDA_TRY(cudaMemcpyAsync(ok, dok.p, count, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return VOSS_OK;
+}
+
+VOSS_API int voss_probe_smem_rmw(voss_ctx* c, double* gbs) {
+  if (!c || !gbs) return fail(VOSS_ERR_ARG, "NULL argument");
+  cudaSetDevice(c->device);
+  float ms = 0;
+  double bytes = 0;
+  if (probe_smem_rmw(c->sm_count, c->stream, &ms, &bytes)) return fail(VOSS_ERR_CUDA, "probe failed");
+  *gbs = bytes / (ms * 1e-3) / 1e9;
+  return VOSS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,354 @@
+#!/usr/bin/env python3
+"""Benchmark: wheel-30 sieve + fused gap statistics of [1, 10^12] on B200.
+
+Workload (one "step"): sieve every integer of [1, N] (N = 10^12 by default) and compute the
+reference's statistics in reference-compat mode: pi(N), the gap histogram, mod-4 / mod-q
+counts, the per-residue gap histogram, the large-gap list and the maximal gap.  Metric:
+range/s = integers sieved per second (higher is better).
+
+  value      device time of the sieve+stitch+reduce kernels per step (CUDA events on the
+             launching stream, L2 flushed between steps outside the timed events), max over
+             ranks; inputs (base-prime table) resident in HBM.
+  e2e        the same step through the public C ABI call voss_sieve_range with host result
+             buffers (device->host copy of the statistics and large-gap list inside the
+             timed region), wall clock, max over ranks; for N > 1 it includes the NCCL
+             all-gather of the per-rank statistics and their merge on rank 0.
+  roofline   dominant kernel sieve_tiles_kernel against the device's measured shared-memory
+             read-modify-write bandwidth (the sieve never touches HBM).
+  cpu_baseline  the oracle's OpenMP interval sieve (a restatement of the reference's
+             verify_cpp marking loop) on a bounded sample of the same range, rank 0, N = 1.
+  ref_cuda   the reference's voss_v7_live.cu rebuilt for sm_100a (oracle/_ref), its printed
+             TOTAL TIME at the same N (rank 0, N = 1), when the binary is present.
+
+Multi-GPU (torchrun): weak scaling; rank r sieves [r*N + 1, (r+1)*N], the statistics are
+all-gathered over NCCL and merged (voss_stats_merge) into those of [1, world*N].
+
+`--impl reference` times the reference's CPU path for this workload (see cpu_baseline) and
+prints the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "voss-prime-gaps_v1_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+SEG_NUM = 30_000_000_000
+METRIC = "range/s sieved to 1e12 (sieve + fused gap/mod-q statistics)"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=10**12)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU sample duration")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(p))
+    except (OSError, ValueError):
+        return {}
+
+
+def profile_traffic_per_unit() -> tuple[float | None, str | None]:
+    """DRAM bytes per sieved integer of sieve_tiles_kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "sieve_tiles_kernel_1e11.md")
+    try:
+        txt = open(p).read()
+    except OSError:
+        return None, None
+    m = re.search(r"dram_bytes_per_integer:\s*([0-9.eE+-]+)", txt)
+    return (float(m.group(1)), p) if m else (None, None)
+
+
+# ---------------------------------------------------------------------------------------
+def cpu_baseline(n: int, seconds: float, ranges_done=None) -> dict:
+    """Oracle OpenMP interval sieve (port of verify_cpp's marking loop) on the top of [1, n]."""
+    import oracle_lib as O
+    threads = O.oracle().oracle_max_threads()
+    probe = 2 * 10**8
+    lo = max(1, n + 1 - probe)
+    t0 = time.perf_counter()
+    O.sieve_range(lo, n + 1, compat=True, seg_num=SEG_NUM, threads=threads)
+    dt = time.perf_counter() - t0
+    rate = (n + 1 - lo) / max(dt, 1e-6)
+    span = int(min(n, max(probe, rate * seconds)))
+    lo = max(1, n + 1 - span)
+    t0 = time.perf_counter()
+    O.sieve_range(lo, n + 1, compat=True, seg_num=SEG_NUM, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": (n + 1 - lo) / dt, "unit": "range/s", "cores": threads, "kind": "port",
+            "sample": f"oracle interval sieve + statistics of [{lo}, {n}] ({n + 1 - lo:.3e} integers, "
+                      f"{dt:.1f} s, OpenMP {threads} threads)"}
+
+
+def ref_cuda_baseline(n: int) -> dict | None:
+    exe = os.path.join(ROOT, "oracle", "_ref", f"voss_v7_live_{n}")
+    if not os.path.exists(exe):
+        return None
+    with tempfile.TemporaryDirectory(prefix="voss_ref_run_") as d:
+        t0 = time.perf_counter()
+        r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=900)
+        wall = time.perf_counter() - t0
+    m = re.search(r"TOTAL TIME:\s*([0-9.]+)\s*s", r.stdout)
+    pi = re.search(r"Total primes:\s*(\d+)", r.stdout)
+    if r.returncode != 0 or not m:
+        return {"unavailable": f"reference binary rc={r.returncode}"}
+    t = float(m.group(1))
+    return {"value": n / t, "unit": "range/s", "total_time_s": t, "wall_s": round(wall, 2),
+            "pi": int(pi.group(1)) if pi else None,
+            "what": "reference src/voss_v7_live.cu rebuilt with nvcc -O3 -arch=sm_100a, its TOTAL TIME"}
+
+
+# ---------------------------------------------------------------------------------------
+def run_reference_arm(a) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle_lib as O
+    threads = O.oracle().oracle_max_threads()
+    # size one step as a bounded sample (about 4 s) of the top of [1, n]
+    probe = 10**8
+    lo = a.n + 1 - probe
+    t0 = time.perf_counter()
+    O.sieve_range(lo, a.n + 1, compat=True, seg_num=SEG_NUM, threads=threads)
+    rate = probe / (time.perf_counter() - t0)
+    span = int(min(a.n, max(probe, rate * 4.0)))
+    lo = a.n + 1 - span
+    for _ in range(a.warmup):
+        O.sieve_range(lo, a.n + 1, compat=True, seg_num=SEG_NUM, threads=threads)
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        O.sieve_range(lo, a.n + 1, compat=True, seg_num=SEG_NUM, threads=threads)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * statistics.mean(times)
+    value = span / (ms * 1e-3)
+    sample = f"oracle interval sieve + statistics of [{lo}, {a.n}] per step ({span:.3e} integers)"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "range/s", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (integer range)",
+        "config": {"workload": f"sieve+stats of [1, {a.n}] (bounded CPU sample)", "n": a.n, "seg_num": SEG_NUM},
+        "cpu_baseline": {"value": value, "unit": "range/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "range/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference_arm(a)
+        return
+    import numpy as np
+    import torch
+    import voss
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+    n = a.n
+    lo, hi = rank * n + 1, (rank + 1) * n + 1
+    ctx = voss.Context(world * n + 1, device=local)
+    stream = torch.cuda.Stream(device=local)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+
+    # warm-up (W untimed steps)
+    for _ in range(a.warmup):
+        with torch.cuda.stream(stream):
+            ctx.sieve_range_device(lo, hi, compat=True, seg_num=SEG_NUM, stream=stream.cuda_stream)
+        stream.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    # ---- value: device-resident steps ----------------------------------------------------
+    barrier()
+    sieve_ms = []
+    for k in range(a.steps):
+        with torch.cuda.stream(stream):
+            flush.add_(1)  # write > L2 between steps, outside the timed events
+            ev[k][0].record(stream)
+            ctx.sieve_range_device(lo, hi, compat=True, seg_num=SEG_NUM, stream=stream.cuda_stream)
+            ev[k][1].record(stream)
+        stream.synchronize()
+        sieve_ms.append(ctx.last_kernel_ms()[0])
+    barrier()
+    step_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+    kernel_ms = statistics.mean(sieve_ms)
+    # ---- e2e: through the public C ABI with host buffers ---------------------------------
+    barrier()
+    t0 = time.perf_counter()
+    last = None
+    for k in range(a.steps):
+        r = ctx.sieve_range(lo, hi, compat=True, seg_num=SEG_NUM)
+        if world > 1:
+            blob = torch.frombuffer(bytearray(bytes(r.raw)), dtype=torch.uint8).to(f"cuda:{local}")
+            gathered = [torch.empty_like(blob) for _ in range(world)]
+            dist.all_gather(gathered, blob)
+            if rank == 0:
+                parts = []
+                for gt in gathered:
+                    st = voss._native.RangeStats.from_buffer_copy(gt.cpu().numpy().tobytes())
+                    parts.append(voss.range_result(st))
+                merged = voss.merge_stats(parts)
+                last = merged
+        else:
+            last = r
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / a.steps
+    barrier()
+    clk = clocks.stop()
+
+    t_step = torch.tensor([step_ms, e2e_s, kernel_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t_step, op=dist.ReduceOp.MAX)
+    step_ms, e2e_s, kernel_ms = t_step.tolist()
+
+    if rank != 0:
+        del ctx
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    total_range = world * n
+    value = total_range / (step_ms * 1e-3)
+    # algorithmic bytes of the dominant kernel: 8 B per bit-clear (32-bit RMW) + one read of
+    # the bitmap (N/30 B) by the extraction, for this rank's range
+    import oracle_lib as O
+    h = O.sieve_work(hi - 1) - (O.sieve_work(lo - 1) if lo > 1 else 0)
+    alg_bytes = 8.0 * h + (hi - lo) / 30.0
+    smem_peak = ctx.probe_smem_rmw()
+    achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    tpu, tsrc = profile_traffic_per_unit()
+    peaks = measured_peaks()
+    r = last
+    d2h = 32 + 32 + 2800 * 8 + 16 * int(min(r.large_total, 1 << 22)) if r is not None else 0
+    out = {
+        "metric": METRIC, "value": value, "unit": "range/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (the integer range itself)",
+        "config": {"workload": f"wheel-30 sieve + reference statistics of [1, {n}] per GPU "
+                               f"(REF_COMPAT, SEG_NUM={SEG_NUM})", "n_per_gpu": n,
+                   "range": [1, total_range], "l2": "flushed (256 MiB write) between timed steps",
+                   "tuning": ctx.tuning(), "parallelism": f"range-sharded x{world}"},
+        "e2e": {"value": total_range / e2e_s, "unit": "range/s", "h2d_bytes_per_step": 48,
+                "d2h_bytes_per_step": d2h, "api": "voss_sieve_range (host buffers)"},
+        "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
+                     "frac": achieved / smem_peak, "traffic": (tpu * (hi - lo)) if tpu else None,
+                     "kernel": "sieve_tiles_kernel", "kernel_ms": kernel_ms,
+                     "algorithmic_bytes": alg_bytes, "bit_clears": h,
+                     "peak_source": "voss_probe_smem_rmw: bank-conflict-free shared-memory atomicAnd on "
+                                    "this GPU in this run (8 B per 32-bit RMW); MEASURED_PEAKS.json has no "
+                                    "shared-memory entry",
+                     "hbm_peak_measured_gbs": peaks.get("hbm_gbs"),
+                     "traffic_source": tsrc},
+        "clocks": clk,
+        "gpu_launches": 3 * a.steps,
+        "result": {"pi": r.prime_count if r else None, "max_gap": r.max_gap if r else None,
+                   "large_gaps": r.large_total if r else None},
+    }
+    if world == 1:
+        if not a.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(n, a.cpu_seconds)
+        if not a.no_ref_cuda:
+            rc = ref_cuda_baseline(n)
+            if rc is not None:
+                out["ref_cuda"] = rc
+    print(json.dumps(out), flush=True)
+    del ctx
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

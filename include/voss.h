@@ -118,7 +118,8 @@ typedef struct voss_tuning {
   uint32_t ctas_per_sm;     /* resident tiles per SM */
   uint32_t coop_div;        /* primes p < tile_bytes/coop_div are cleared warp-cooperatively */
   uint32_t mult_factor;     /* primes p >= mult_factor*tile_bytes use the multiples walk */
-  uint32_t reserved[3];
+  uint32_t medium_mode;     /* other primes: 0 = a thread per prime, 1 = a lane per (prime, residue) */
+  uint32_t reserved[2];
 } voss_tuning;
 
 typedef struct voss_ctx voss_ctx;

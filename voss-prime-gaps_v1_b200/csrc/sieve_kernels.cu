@@ -126,13 +126,28 @@ __device__ __forceinline__ uint32_t pre_off(int g) {
   return g == 0 ? 0u : (g == 1 ? 1001u : (g == 2 ? 1324u : 1991u));
 }
 
+#ifdef VOSS_PHASE_TIMING
+// Instrumented build only: per-phase cycles summed over all CTAs (thread 0 of each CTA
+// timestamps every phase boundary after a block barrier).
+__device__ unsigned long long g_phase_cycles[16];
+#define VOSS_PHASE(k)                                  \
+  __syncthreads();                                     \
+  if (threadIdx.x == 0) {                              \
+    const long long now__ = clock64();                 \
+    ph_acc[(k)] += (unsigned long long)(now__ - ph_t); \
+    ph_t = now__;                                      \
+  }
+#else
+#define VOSS_PHASE(k)
+#endif
+
 struct TileHdr {
   unsigned long long ktile, vbase, vlo, vhi, seg_k;
   uint32_t nw, lt, np, ia, ib, vb, gthr, k28, k143;
   uint32_t pre_base[kPreGroups];
   uint32_t interval, tile, next_tile, cur_iv, since_flush, flush;
   uint32_t r0, r1;       // base primes lying in the tile (restore)
-  uint32_t coop_ctr;
+  uint32_t coop_ctr, b_ctr, c_ctr;  // work counters of the three prime categories
   uint32_t first;
   uint32_t tile_base_rank;
   unsigned long long count_total;
@@ -256,10 +271,16 @@ sieve_tiles_kernel(SieveArgs a) {
   uint32_t* cnt = pre + kPreWords;
   __shared__ TileHdr H;
   __shared__ BlockScratch<BLOCK> S;
+  // Wheel tables in shared memory: lanes index them by their own prime's residue, which
+  // would serialize in the constant cache.
+  __shared__ uint8_t s_step[64];
+  __shared__ int8_t s_rb[32];
   uint32_t* err = a.error;
 
   const int tid = threadIdx.x, lane = tid & 31;
   for (uint32_t i = tid; i < kPreWords; i += BLOCK) pre[i] = a.pretab[i];
+  if (tid < 64) s_step[tid] = c_wheel_step[tid];
+  if (tid < 32) s_rb[tid] = c_res_bit[tid];
   if (!EMIT)
     for (uint32_t i = tid; i < (uint32_t)kSmCounters; i += BLOCK) cnt[i] = 0;
   if (tid == 0) {
@@ -271,6 +292,10 @@ sieve_tiles_kernel(SieveArgs a) {
   __syncthreads();
 
   const uint32_t C = a.chunk_words;
+#ifdef VOSS_PHASE_TIMING
+  unsigned long long ph_acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  long long ph_t = clock64();
+#endif
 
   for (;;) {
     // ---- claim / flush ------------------------------------------------------------------
@@ -300,6 +325,7 @@ sieve_tiles_kernel(SieveArgs a) {
       __syncthreads();
     }
     if (H.tile >= a.n_tiles) break;
+    VOSS_PHASE(0)
 
     // ---- tile header ------------------------------------------------------------------
     if (tid == 0) {
@@ -342,9 +368,12 @@ sieve_tiles_kernel(SieveArgs a) {
 #pragma unroll
       for (int g = 0; g < kPreGroups; ++g) H.pre_base[g] = (uint32_t)(wt % pre_mod(g));
       H.coop_ctr = 0;
+      H.b_ctr = 0;
+      H.c_ctr = 0;
       H.first = kNone;
     }
     __syncthreads();
+    VOSS_PHASE(1)
 
     const uint32_t nw = H.nw, Lt = H.lt;
 
@@ -373,6 +402,7 @@ sieve_tiles_kernel(SieveArgs a) {
       }
     }
     __syncthreads();
+    VOSS_PHASE(2)
 
     // ---- 2. sieve ----------------------------------------------------------------------
     {
@@ -386,11 +416,11 @@ sieve_tiles_kernel(SieveArgs a) {
         if (i >= ia) break;
         const uint32_t p = a.primes[i];
         const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
-        const uint32_t pa = p / 30u, bi = (uint32_t)c_res_bit[p - 30u * pa];
+        const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
         const uint32_t stride = 32u * p;
 #pragma unroll 1
         for (uint32_t o = 0; o < 8; ++o) {
-          const uint32_t e = c_wheel_step[bi * 8u + o];
+          const uint32_t e = s_step[bi * 8u + o];
           const uint32_t delta = pa * w30(o) + (e & 31u);
           uint32_t s = delta >= r ? delta - r : delta + p - r;
           uint32_t byte = s + (uint32_t)lane * p;
@@ -398,36 +428,76 @@ sieve_tiles_kernel(SieveArgs a) {
           for (; byte < Lt; byte += stride) clear_bit_word(bm, byte >> 2, mask, nw, err);
         }
       }
-      // medium primes: a thread per prime, 8 residue progressions
-      for (uint32_t i = ia + tid; i < ib; i += BLOCK) {
-        const uint32_t p = a.primes[i];
-        const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
-        const uint32_t pa = p / 30u, bi = (uint32_t)c_res_bit[p - 30u * pa];
+      VOSS_PHASE(3)
+      // medium primes
+      if (a.b_mode == 0) {
+        // a thread per prime, 8 residue progressions; warps claim 32 consecutive primes at a time
+        for (;;) {
+          uint32_t base = 0;
+          if (lane == 0) base = atomicAdd(&H.b_ctr, 32u);
+          base = __shfl_sync(0xFFFFFFFFu, base, 0);
+          if (base >= ib - ia) break;
+          const uint32_t i = ia + base + (uint32_t)lane;
+          if (i < ib) {
+            const uint32_t p = a.primes[i];
+            const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
+            const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
 #pragma unroll
-        for (uint32_t o = 0; o < 8; ++o) {
-          const uint32_t e = c_wheel_step[bi * 8u + o];
-          const uint32_t delta = pa * w30(o) + (e & 31u);
-          uint32_t byte = delta >= r ? delta - r : delta + p - r;
-          const uint32_t bit = e >> 5;
-          for (; byte < Lt; byte += p)
-            clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
+            for (uint32_t o = 0; o < 8; ++o) {
+              const uint32_t e = s_step[bi * 8u + o];
+              const uint32_t delta = pa * w30(o) + (e & 31u);
+              uint32_t byte = delta >= r ? delta - r : delta + p - r;
+              const uint32_t bit = e >> 5;
+              for (; byte < Lt; byte += p)
+                clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
+            }
+          }
+        }
+      } else {
+        // a lane per (prime, residue): a warp takes 4 consecutive primes, lane = 8*prime + residue
+        const uint32_t o = (uint32_t)lane & 7u;
+        const uint32_t wo = w30(o);
+        const uint32_t groups = (ib - ia + 3u) >> 2;
+        const uint32_t warp = (uint32_t)tid >> 5;
+        for (uint32_t g = warp; g < groups; g += BLOCK / 32) {
+          const uint32_t i = ia + 4u * g + ((uint32_t)lane >> 3);
+          if (i < ib) {
+            const uint32_t p = a.primes[i];
+            const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
+            const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
+            const uint32_t e = s_step[bi * 8u + o];
+            const uint32_t delta = pa * wo + (e & 31u);
+            uint32_t byte = delta >= r ? delta - r : delta + p - r;
+            const uint32_t bit = e >> 5;
+            for (; byte < Lt; byte += p)
+              clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
+          }
         }
       }
+      VOSS_PHASE(4)
       // large primes: walk the multiples of p across the tile's span of integers
       const uint64_t vbase = H.vbase;
       const uint32_t span = 30u * Lt;
-      for (uint32_t i = ib + tid; i < np; i += BLOCK) {
-        const uint32_t p = a.primes[i];
-        const uint32_t r = mod_barrett(vbase, p, a.magic[i]);
-        uint32_t d = r ? p - r : 0u;
-        for (; d < span; d += p) {
-          const uint32_t q = d / 30u;
-          const int b = c_res_bit[d - 30u * q];
-          if (b >= 0) clear_bit_word(bm, q >> 2, ~(1u << (((q & 3u) << 3) | (uint32_t)b)), nw, err);
+      for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&H.c_ctr, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= np - ib) break;
+        const uint32_t i = ib + base + (uint32_t)lane;
+        if (i < np) {
+          const uint32_t p = a.primes[i];
+          const uint32_t r = mod_barrett(vbase, p, a.magic[i]);
+          uint32_t d = r ? p - r : 0u;
+          for (; d < span; d += p) {
+            const uint32_t q = d / 30u;
+            const int b = s_rb[d - 30u * q];
+            if (b >= 0) clear_bit_word(bm, q >> 2, ~(1u << (((q & 3u) << 3) | (uint32_t)b)), nw, err);
+          }
         }
       }
     }
     __syncthreads();
+    VOSS_PHASE(5)
 
     // ---- 3. restore primes lying in the tile ---------------------------------------------
     {
@@ -437,7 +507,7 @@ sieve_tiles_kernel(SieveArgs a) {
         const uint64_t p = sp[tid];
         if (p >= vlo && p < vhi && p >= vbase && p < vend) {
           const uint32_t off = (uint32_t)(p - vbase), k = off / 30u;
-          atomicOr(bm + (k >> 2), 1u << (((k & 3u) << 3) | (uint32_t)c_res_bit[off - 30u * k]));
+          atomicOr(bm + (k >> 2), 1u << (((k & 3u) << 3) | (uint32_t)s_rb[off - 30u * k]));
         }
       }
       for (uint32_t i = H.r0 + tid; i < H.r1; i += BLOCK) {
@@ -445,11 +515,12 @@ sieve_tiles_kernel(SieveArgs a) {
         if (p >= vlo && p < vhi && p >= vbase && p < vend) {
           const uint32_t off = (uint32_t)(p - vbase), k = off / 30u;
           if ((k >> 2) < nw)
-            atomicOr(bm + (k >> 2), 1u << (((k & 3u) << 3) | (uint32_t)c_res_bit[off - 30u * k]));
+            atomicOr(bm + (k >> 2), 1u << (((k & 3u) << 3) | (uint32_t)s_rb[off - 30u * k]));
         }
       }
     }
     __syncthreads();
+    VOSS_PHASE(6)
 
     // ---- 4. extract -----------------------------------------------------------------------
     const uint32_t c0 = (uint32_t)tid * C;
@@ -487,6 +558,7 @@ sieve_tiles_kernel(SieveArgs a) {
       }
       int32_t tile_last;
       int32_t prev = block_excl_max<BLOCK>(my_last, S, &tile_last);
+      VOSS_PHASE(7)
 
       // pass 2: walk the chunk in order
       const uint32_t vb = H.vb;
@@ -497,7 +569,7 @@ sieve_tiles_kernel(SieveArgs a) {
       uint32_t o_prev = 0;
       if (prev >= 0) {
         const uint32_t kp = (uint32_t)prev / 30u;
-        o_prev = (uint32_t)c_res_bit[(uint32_t)prev - 30u * kp];
+        o_prev = (uint32_t)s_rb[(uint32_t)prev - 30u * kp];
       }
       uint32_t w = c0;
       uint32_t x = w < cend ? bm[w] : 0u;
@@ -561,6 +633,7 @@ sieve_tiles_kernel(SieveArgs a) {
       uint32_t tile_cnt;
       unsigned long long tile_key;
       __syncthreads();  // H.first visible, scratch reuse
+      VOSS_PHASE(8)
       block_reduce_tile<BLOCK>(my_cnt, key, S, &tile_cnt, &tile_key);
       if (tid == 0) {
         TilePartial P;
@@ -578,7 +651,12 @@ sieve_tiles_kernel(SieveArgs a) {
     }
     if (tid == 0) H.next_tile = atomicAdd(a.tile_counter, 1u);
     __syncthreads();
+    VOSS_PHASE(9)
   }
+#ifdef VOSS_PHASE_TIMING
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 10; ++k) atomicAdd(&g_phase_cycles[k], ph_acc[k]);
+#endif
 }
 
 // Gap between the last prime of the previous non-empty tile and this tile's first prime.
@@ -705,6 +783,18 @@ __global__ void __launch_bounds__(1024) smem_rmw_probe_kernel(uint32_t* sink) {
 }
 
 // ---- host side ------------------------------------------------------------------------------
+#ifdef VOSS_PHASE_TIMING
+int read_phase_cycles(unsigned long long* out, int n, bool reset) {
+  unsigned long long h[16];
+  if (cudaMemcpyFromSymbol(h, g_phase_cycles, sizeof(h)) != cudaSuccess) return -1;
+  for (int i = 0; i < n && i < 16; ++i) out[i] = h[i];
+  if (reset) {
+    unsigned long long z[16] = {0};
+    if (cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z)) != cudaSuccess) return -1;
+  }
+  return 0;
+}
+#endif
 static const int kW30h[8] = {1, 7, 11, 13, 17, 19, 23, 29};
 
 static int ensure_tables() {

@@ -154,10 +154,11 @@ int apply_tuning(voss_ctx* c, const voss_tuning& t0) {
   voss_tuning t = t0;
   if (!t.block_threads) t.block_threads = 1024;
   if (!t.chunk_words) t.chunk_words = t.block_threads == 1024 ? 49 : 45;
-  if (!t.coop_div) t.coop_div = 32;
+  if (!t.coop_div) t.coop_div = 48;
   if (!t.mult_factor) t.mult_factor = 8;
   if (t.block_threads != 512 && t.block_threads != 1024)
     return fail(VOSS_ERR_ARG, "block_threads must be 512 or 1024");
+  if (t.medium_mode > 1) return fail(VOSS_ERR_ARG, "medium_mode must be 0 or 1");
   if ((t.chunk_words & 1u) == 0 || t.chunk_words > 255)
     return fail(VOSS_ERR_ARG, "chunk_words must be odd and <= 255");
   const uint32_t tw = t.block_threads * t.chunk_words;
@@ -243,6 +244,7 @@ int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_c
   a.coop_div = c->tune.coop_div;
   a.mult_factor = c->tune.mult_factor;
   a.want_large = want_large ? 1u : 0u;
+  a.b_mode = c->tune.medium_mode;
   uint32_t* ctr = W.counters.as<uint32_t>();
   a.tile_counter = ctr + kCtrTile;
   a.large_count = ctr + kCtrLarge;
@@ -607,8 +609,13 @@ VOSS_API int voss_sieve_range(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t fl
 
 VOSS_API int voss_last_kernel_ms(const voss_ctx* c, double* sieve_ms, double* total_ms) {
   if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
-  if (sieve_ms) *sieve_ms = c->sieve_ms;
-  if (total_ms) *total_ms = c->total_ms;
+  cudaSetDevice(c->device);
+  float a = 0, b = 0;
+  CUDA_TRY(cudaEventSynchronize(c->ev2));
+  CUDA_TRY(cudaEventElapsedTime(&a, c->ev0, c->ev1));
+  CUDA_TRY(cudaEventElapsedTime(&b, c->ev0, c->ev2));
+  if (sieve_ms) *sieve_ms = a;
+  if (total_ms) *total_ms = b;
   return VOSS_OK;
 }
 
@@ -785,3 +792,13 @@ VOSS_API int voss_probe_smem_rmw(voss_ctx* c, double* gbs) {
 }
 
 }  // extern "C"
+
+#ifdef VOSS_PHASE_TIMING
+namespace voss {
+int read_phase_cycles(unsigned long long* out, int n, bool reset);
+}
+// Instrumented build only (libvoss_timing.so): cycles per kernel phase summed over CTAs.
+extern "C" VOSS_API int voss_debug_phase_cycles(unsigned long long* out, int n, int reset) {
+  return voss::read_phase_cycles(out, n, reset != 0) ? VOSS_ERR_CUDA : VOSS_OK;
+}
+#endif

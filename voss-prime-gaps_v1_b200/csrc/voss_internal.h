@@ -107,6 +107,7 @@ struct SieveArgs {
   uint32_t coop_div;
   uint32_t mult_factor;
   uint32_t want_large;      // record large gaps
+  uint32_t b_mode;          // medium primes: 0 = thread per prime, 1 = lane per (prime, residue)
   uint32_t* tile_counter;
   TilePartial* partials;
   unsigned long long* acc;  // n_intervals * kAccStride

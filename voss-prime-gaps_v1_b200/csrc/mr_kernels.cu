@@ -14,6 +14,7 @@
 // to a work list; mr_finish_kernel runs the remaining eleven bases on that list.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "voss_internal.h"
@@ -23,7 +24,8 @@ namespace voss {
 __constant__ uint64_t c_base_inv[12];  // B^-1 mod 2^64 (odd B), for the divisibility test
 __constant__ uint64_t c_base_lim[12];  // floor((2^64-1)/B)
 
-static bool g_mr_ready = false;
+// Constant memory is per device: the tables are uploaded once for each device ordinal.
+static std::atomic<uint64_t> g_mr_ready{0};
 static const uint64_t kBases[12] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
 
 struct Mont {
@@ -166,7 +168,7 @@ __global__ void mr_sieve_kernel(const uint64_t* __restrict__ cand, uint64_t coun
   }
 }
 
-// `work` holds indices < 2^32; candidates beyond that are handled by mr_direct_kernel.
+// `work` holds candidate indices (< 2^32: the entry points take fewer than 2^32 candidates per call).
 __global__ void mr_finish_kernel(const uint64_t* __restrict__ cand, uint8_t* __restrict__ out,
                                  const uint32_t* __restrict__ work, const uint32_t* __restrict__ nwork) {
   const uint32_t nw = *nwork;
@@ -232,7 +234,10 @@ __global__ void prove_gaps_kernel(const uint64_t* __restrict__ p_after, const in
 }
 
 static int ensure_mr_tables() {
-  if (g_mr_ready) return 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+  const uint64_t bit = 1ull << dev;
+  if (g_mr_ready.load() & bit) return 0;
   uint64_t inv[12], lim[12];
   for (int i = 0; i < 12; ++i) {
     const uint64_t b = kBases[i];
@@ -247,7 +252,7 @@ static int ensure_mr_tables() {
   }
   if (cudaMemcpyToSymbol(c_base_inv, inv, sizeof(inv)) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_base_lim, lim, sizeof(lim)) != cudaSuccess) return -1;
-  g_mr_ready = true;
+  g_mr_ready.fetch_or(bit);
   return 0;
 }
 

@@ -23,6 +23,7 @@
 // first/last prime and maximal gap.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 
@@ -36,7 +37,8 @@ __constant__ uint8_t c_wheel_step[64];
 // residue r (mod 30) -> wheel bit index, or -1 when gcd(r, 30) > 1.
 __constant__ int8_t c_res_bit[32];
 
-static bool g_tables_ready = false;
+// Constant memory is per device: the tables are uploaded once for each device ordinal.
+static std::atomic<uint64_t> g_tables_ready{0};
 
 __device__ __forceinline__ uint32_t w30(uint32_t o) {
   return (uint32_t)((kW30Packed >> (8u * o)) & 0xFFu);
@@ -798,7 +800,10 @@ int read_phase_cycles(unsigned long long* out, int n, bool reset) {
 static const int kW30h[8] = {1, 7, 11, 13, 17, 19, 23, 29};
 
 static int ensure_tables() {
-  if (g_tables_ready) return 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+  const uint64_t bit = 1ull << dev;
+  if (g_tables_ready.load() & bit) return 0;
   uint8_t step[64];
   int8_t rb[32];
   for (int r = 0; r < 32; ++r) rb[r] = -1;
@@ -810,7 +815,7 @@ static int ensure_tables() {
     }
   if (cudaMemcpyToSymbol(c_wheel_step, step, sizeof(step)) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_res_bit, rb, sizeof(rb)) != cudaSuccess) return -1;
-  g_tables_ready = true;
+  g_tables_ready.fetch_or(bit);
   return 0;
 }
 

@@ -178,6 +178,22 @@ VOSS_API int voss_mr_verify(voss_ctx* ctx, const uint64_t* n, uint64_t count, ui
 /* Device pointers; `stream` as for voss_sieve_range_device. */
 VOSS_API int voss_mr_verify_device(voss_ctx* ctx, const uint64_t* d_n, uint64_t count,
                                    uint8_t* d_is_prime, void* stream);
+/* The same verdicts as voss_mr_verify_device, for callers that cannot allocate device memory
+ * during the call: processes whose device memory is already reserved by another allocator (a
+ * framework's caching allocator or a memory pool), and service request paths where
+ * cudaMalloc/cudaFree would synchronize the device.  No counterpart in the reference.
+ * It takes no context and allocates nothing: its scratch is a fixed array inside libvoss.so
+ * (16 MiB, held on every device that loads the library until exit), so
+ *   - count may not exceed 4194304 (1 << 22) per call; larger counts return VOSS_ERR_ARG;
+ *   - every call shares that array: calls that overlap on the GPU (different streams, or
+ *     different host threads on one device) race; order them on one stream;
+ *   - the first call on a device sets up (looks up the array's device address and uploads the
+ *     Miller-Rabin constant tables) on the calling thread's current device; make that first
+ *     call before any stream capture.
+ * d_n and d_is_prime are device pointers on the current device; `stream` is a cudaStream_t or
+ * NULL for the legacy default stream.  The call is asynchronous on `stream`. */
+VOSS_API int voss_mr_verify_noalloc(const uint64_t* d_n, uint64_t count, uint8_t* d_is_prime,
+                                    void* stream);
 /* ok[i] = verify_gap(p_after[i], gap[i]) of src/verify_cpp.cpp:59-93: both ends prime and
  * every interior integer marked by the reference's interval sieve. */
 VOSS_API int voss_prove_gaps(voss_ctx* ctx, const uint64_t* p_after, const int32_t* gap,

@@ -16,6 +16,10 @@
 
 #include <atomic>
 #include <cstdint>
+#include <cstdio>
+#include <mutex>
+
+#include "voss.h"
 
 #include "voss_internal.h"
 
@@ -284,3 +288,77 @@ int launch_prove_gaps(const uint64_t* d_p_after, const int32_t* d_gap, uint64_t 
 }
 
 }  // namespace voss
+
+// =====================================================================================
+// Miller-Rabin without any allocation (voss_mr_verify_noalloc).
+//
+// Some callers cannot allocate device memory at call time: a process whose device memory is
+// already reserved by another allocator (a framework's caching allocator or a memory pool),
+// where cudaMalloc would fail or fragment that pool, and request paths of long-running
+// services, where cudaMalloc/cudaFree would synchronize the device and stall other streams.
+// The regular entry points allocate (the context at creation, per-call buffers on growth);
+// this one needs no context and allocates nothing: its scratch (the survivor work list and
+// its counter) is the fixed array below, which every device that loads libvoss.so holds
+// until the process exits.
+// =====================================================================================
+namespace voss {
+
+constexpr uint64_t kNoAllocMaxCount = 1ull << 22;  // candidates per call (16 MiB of scratch)
+constexpr uint32_t kNoAllocListOffset = 64;         // counter at [0]; list starts 256 B in
+
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocMaxCount + kNoAllocListOffset];
+
+static std::mutex g_noalloc_mu;
+static uint32_t* g_noalloc_ptr[64];  // device address of g_noalloc_scratch, per device ordinal
+static int g_noalloc_sms[64];
+
+}  // namespace voss
+
+namespace voss_detail {
+int set_error(int code, const char* msg);
+}
+
+extern "C" VOSS_API int voss_mr_verify_noalloc(const uint64_t* d_n, uint64_t count, uint8_t* d_is_prime,
+                                               void* stream) {
+  using namespace voss;
+  char msg[160];
+  if (count == 0) return VOSS_OK;
+  if (!d_n || !d_is_prime) return voss_detail::set_error(VOSS_ERR_ARG, "NULL device pointer");
+  if (count > kNoAllocMaxCount) {
+    snprintf(msg, sizeof(msg), "count %llu exceeds the no-allocation limit of %llu candidates per call",
+             (unsigned long long)count, (unsigned long long)kNoAllocMaxCount);
+    return voss_detail::set_error(VOSS_ERR_ARG, msg);
+  }
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return voss_detail::set_error(VOSS_ERR_NODEV, "no current CUDA device");
+  uint32_t* scratch = nullptr;
+  int sms = 0;
+  {
+    // set-up, once per device, on the calling thread's current device: the host-side name of
+    // the array is not a device address, so the kernel gets the address the runtime reports
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p) {
+        snprintf(msg, sizeof(msg), "cudaGetSymbolAddress(no-allocation scratch) failed: %s", cudaGetErrorString(e));
+        return voss_detail::set_error(VOSS_ERR_CUDA, msg);
+      }
+      int n = 0;
+      if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+        return voss_detail::set_error(VOSS_ERR_CUDA, "cannot read the SM count");
+      g_noalloc_ptr[dev] = static_cast<uint32_t*>(p);
+      g_noalloc_sms[dev] = n;
+    }
+    scratch = g_noalloc_ptr[dev];
+    sms = g_noalloc_sms[dev];
+  }
+  // launch_mr clears the counter (cudaMemsetAsync on `scratch`) before its kernels; the list
+  // needs no clearing since entries are written before they are read.
+  if (launch_mr(d_n, count, d_is_prime, scratch + kNoAllocListOffset, scratch, stream, sms) != 0) {
+    snprintf(msg, sizeof(msg), "Miller-Rabin launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return voss_detail::set_error(VOSS_ERR_CUDA, msg);
+  }
+  return VOSS_OK;
+}

@@ -234,6 +234,16 @@ def merge_stats(parts: list[RangeResult], large_cap: int | None = None) -> Range
     return range_result(out, large[: w.value].copy())
 
 
+NOALLOC_MAX_COUNT = 1 << 22
+
+
+def mr_verify_noalloc(d_n: int, count: int, d_is_prime: int, stream: int = 0) -> None:
+    """voss_mr_verify_noalloc: Miller-Rabin verdicts into device memory without allocating
+    anything (no context; scratch is a fixed array inside the library, at most
+    NOALLOC_MAX_COUNT candidates per call, calls must not overlap on the GPU)."""
+    N.check(N.load().voss_mr_verify_noalloc(c_void_p(d_n), count, c_void_p(d_is_prime), c_void_p(stream or None)))
+
+
 def device_count() -> int:
     n = c_int()
     N.check(N.load().voss_device_count(byref(n)))

@@ -1,0 +1,149 @@
+"""Pins the CPU oracle (oracle/liboracle.so) to the reference's known answers and to the
+reference verifier compiled unmodified (oracle/_ref/libref_verify.so).  CPU only."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")))
+SEG = 30_000_000_000
+
+
+def brute_primes(n):
+    s = np.ones(n + 1, dtype=bool)
+    s[:2] = False
+    for i in range(2, int(n**0.5) + 1):
+        if s[i]:
+            s[i * i::i] = False
+    return np.nonzero(s)[0].astype(np.uint64)
+
+
+def brute_stats(lo, hi, compat, seg):
+    """Pure-Python statement of the reference's per-pair rules (voss_v7_live.cu:278-299,
+    :551-562, :634-635, :682), for small ranges."""
+    ps = [int(p) for p in brute_primes(max(hi, 2)) if lo <= p < hi]
+    W = [1, 7, 11, 13, 17, 19, 23, 29]
+    hist, modq_gap, large = {}, {}, []
+    mod4 = [0, 0]
+    for p in ps:
+        if p % 4 == 1:
+            mod4[0] += 1
+        elif p % 4 == 3:
+            mod4[1] += 1
+    max_gap, max_lo = 0, 0
+    for a, b in zip(ps, ps[1:]):
+        g = b - a
+        hist[g] = hist.get(g, 0) + 1
+        if g > max_gap:
+            max_gap, max_lo = g, a
+        if a < 7 or (compat and (a - 1) // seg != (b - 1) // seg):
+            continue
+        if g < 100:
+            r6 = 0 if a % 6 == 1 else 1
+            modq_gap[(r6, g)] = modq_gap.get((r6, g), 0) + 1
+            r30 = 2 + W.index(a % 30)
+            modq_gap[(r30, g)] = modq_gap.get((r30, g), 0) + 1
+        merit = g / math.log(a) if g > 100 else 0.0
+        if g >= 500 or merit >= 10.0:
+            large.append((b, g))
+    return dict(count=len(ps), hist=hist, modq_gap=modq_gap, large=large, mod4=mod4, max_gap=max_gap,
+                max_lo=max_lo, first=ps[0] if ps else 0, last=ps[-1] if ps else 0)
+
+
+@pytest.mark.parametrize("n", range(1, 10))
+def test_pi_10n(n):
+    r = O.sieve_range(1, 10**n + 1, compat=True, seg_num=SEG)
+    assert r.prime_count == GOLD["pi_10n"][str(n)]
+    # the reference's three self-checks (voss_v7_live.cu:693-705)
+    gh = r.gap_hist
+    assert int(gh.sum()) == r.prime_count - 1
+    assert int((np.arange(gh.size, dtype=np.uint64) * gh).sum()) == r.last_prime - 2
+    assert int(r.mod4.sum()) + 1 == r.prime_count
+
+
+def test_hist_1000_and_chebyshev_1e9():
+    r = O.sieve_range(1, 1001, compat=True, seg_num=SEG)
+    assert {str(g): int(c) for g, c in enumerate(r.gap_hist) if c} == GOLD["gap_hist"]["1000"]
+    r = O.sieve_range(1, 10**9 + 1, compat=True, seg_num=SEG)
+    assert [int(r.mod4[0]), int(r.mod4[1])] == GOLD["chebyshev"][str(10**9)]
+    assert (r.max_gap, r.max_gap_lo) == (282, 436273009)  # the maximal gap below 1e9
+
+
+def test_sieve_work_matches_baseline_table():
+    assert O.sieve_work(10**9) == 404309576
+    assert O.sieve_work(10**12) == 484385202990
+
+
+@pytest.mark.parametrize("lo,hi,compat,seg", [
+    (1, 20000, True, 30), (1, 20000, True, 330), (1, 50000, True, 30_000_000_000),
+    (1, 20000, False, 0), (2, 3, False, 0), (0, 8, False, 0), (9000, 31000, False, 0),
+    (9000, 31000, True, 990),
+])
+def test_oracle_against_python_statement(lo, hi, compat, seg):
+    r = O.sieve_range(lo, hi, compat=compat, seg_num=seg)
+    b = brute_stats(lo, hi, compat, seg)
+    assert r.prime_count == b["count"]
+    assert (r.first_prime, r.last_prime) == (b["first"], b["last"])
+    assert (r.max_gap, r.max_gap_lo) == (b["max_gap"], b["max_lo"])
+    assert {g: int(c) for g, c in enumerate(r.gap_hist) if c} == b["hist"]
+    got_mg = {(i, g): int(r.modq_gap[i, g]) for i in range(10) for g in range(100) if r.modq_gap[i, g]}
+    assert got_mg == b["modq_gap"]
+    assert sorted(zip(r.large["position"].tolist(), r.large["gap"].tolist())) == sorted(b["large"])
+    assert list(map(int, r.mod4)) == b["mod4"]
+
+
+def test_oracle_modq_counts_small():
+    lo, hi = 1, 30001
+    r = O.sieve_range(lo, hi)
+    ps = brute_primes(hi - 1)
+    for q in (3, 4, 5, 6, 7, 8, 11, 12, 13, 30):
+        want = np.bincount((ps % q).astype(np.int64), minlength=q)
+        np.testing.assert_array_equal(r.modq_counts(q), want)
+
+
+def test_oracle_intervals_and_primes():
+    lo = np.array([0, 1, 2, 100, 10**6, 999_983], dtype=np.uint64)
+    hi = np.array([10, 2, 100, 10**5, 10**6 + 10**4, 999_984], dtype=np.uint64)
+    out = O.sieve_intervals(lo, hi)
+    for i in range(lo.size):
+        ps = [int(p) for p in brute_primes(int(hi[i]) + 1) if lo[i] <= p < hi[i]]
+        assert out["prime_count"][i] == len(ps)
+        gaps = np.diff(np.array(ps, dtype=np.int64))
+        want = np.zeros(1024, dtype=np.uint64)
+        for g in gaps:
+            want[g >> 1] += 1
+        np.testing.assert_array_equal(out["gap_hist"][i], want)
+        np.testing.assert_array_equal(O.primes_range(int(lo[i]), int(hi[i])), np.array(ps, dtype=np.uint64))
+
+
+needs_ref = pytest.mark.skipif(not os.path.exists(O.REF_VERIFY_SO),
+                               reason="oracle/_ref/libref_verify.so not built (reference tree absent)")
+
+SPECIAL = [0, 1, 2, 3, 4, 5, 9, 25, 37, 41, 1369, 2047, 3215031751, 341550071728321, 3825123056546413051,
+           18446744073709551557, 18446744073709551615, 2**61 - 1, 4759123141, 1122004669633]
+
+
+@needs_ref
+def test_mr_port_matches_reference_verifier():
+    rng = np.random.default_rng(5)
+    n = np.concatenate([np.array(SPECIAL, dtype=np.uint64),
+                        rng.integers(0, 2**63, 200_000, dtype=np.uint64) * 2 + 1,
+                        rng.integers(0, 10**6, 50_000, dtype=np.uint64),
+                        brute_primes(200_000)])
+    np.testing.assert_array_equal(O.mr_batch(n), O.ref_mr_batch(n))
+
+
+@needs_ref
+def test_prove_gaps_port_matches_reference_verifier():
+    r = O.sieve_range(1, 10**8 + 1, compat=True, seg_num=SEG)
+    p = r.large["position"].astype(np.uint64)
+    g = r.large["gap"].astype(np.int32)
+    P = np.concatenate([p, p[:40] + 2, np.array([3, 5, 7, 11, 13, 2, 29, 97, 1009, 5], dtype=np.uint64)])
+    G = np.concatenate([g, g[:40], np.array([1, 3, 4, 2, 2, 0, -3, 8, 1006, 2], dtype=np.int32)])
+    want = O.ref_prove_gaps(P, G)
+    np.testing.assert_array_equal(O.prove_gaps(P, G), want)
+    assert want[: p.size].all()

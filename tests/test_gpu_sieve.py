@@ -123,3 +123,30 @@ def test_primes_range_matches_oracle(gpu_ctx):
         g = gpu_ctx.primes_range(lo, hi)
         o = O.primes_range(lo, hi)
         np.testing.assert_array_equal(g, o)
+
+
+def test_high_intervals_match_oracle(gpu_ctx_big):
+    """Intervals up to 10^16 (base primes to 10^8): every prime category, including the
+    multiples walk of primes larger than the tile's span."""
+    rng = np.random.default_rng(20261203)
+    k = 24
+    lo = (np.floor(10 ** rng.uniform(10, 16, k) / 30) * 30).astype(np.uint64)
+    ln = (10 ** rng.uniform(3, 6.3, k)).astype(np.uint64)
+    lo[:3] = [10**16 - 10**6, 10**15, 3 * 10**15 + 7]
+    hi = lo + ln
+    g = gpu_ctx_big.sieve_intervals(lo, hi)
+    o = O.sieve_intervals(lo, hi)
+    for f in ("prime_count", "first_prime", "last_prime", "max_gap", "max_gap_lo", "gap_overflow"):
+        np.testing.assert_array_equal(g[f], o[f], err_msg=f)
+    np.testing.assert_array_equal(g["gap_hist"], o["gap_hist"])
+    for i in (0, 1, 2):
+        gr = gpu_ctx_big.sieve_range(int(lo[i]), int(hi[i]))
+        orr = O.sieve_range(int(lo[i]), int(hi[i]))
+        assert_range_equal(gr, orr)
+
+
+def test_interval_near_1e18(gpu_ctx_big):
+    lo, hi = 10**18 - 2 * 10**5, 10**18 + 10**5
+    g = gpu_ctx_big.sieve_range(lo, hi)
+    o = O.sieve_range(lo, hi)
+    assert_range_equal(g, o)

@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU sample duration")
-    ap.add_argument("--workload", default="range", choices=["range", "intervals"],
+    ap.add_argument("--workload", default="range", choices=["range", "intervals", "mr"],
                     help="range: sieve+stats of [1, n] (headline); intervals: 4096 seeded intervals")
     ap.add_argument("--intervals", type=int, default=4096)
     ap.add_argument("--no-tune", action="store_true")
@@ -265,12 +265,100 @@ def run_intervals(a) -> None:
                    "tuning": ctx.tuning(), "autotune": tune},
         "integers_per_s": total_int / bd,
         "e2e": {"value": lo.size / bw, "unit": "intervals/s", "h2d_bytes_per_step": 48 * int(lo.size),
-                "d2h_bytes_per_step": 8 * 2800 * int(lo.size) + 32 * int(lo.size)},
+                "d2h_bytes_per_step": batched.itemsize * int(lo.size) + 32},
         "plain_launch_per_interval": {"value": lo.size / plain_dev * 1e3, "unit": "intervals/s (device)",
                                       "e2e_value": lo.size / plain_wall, "total_device_ms": plain_dev,
                                       "total_wall_s": plain_wall},
         "speedup_vs_plain": {"device": plain_dev / (bd * 1e3), "e2e": plain_wall / bw},
         "bit_exact_vs_plain": bool(same),
+    }
+    print(json.dumps(out), flush=True)
+
+
+def mr_candidates(ctx, half: int, seed: int = 20261203):
+    """half consecutive primes just below 1e12 (the sieve's own output) + half uniformly random
+    odd 64-bit values (PCG64, fixed seed), interleaved by a seeded permutation."""
+    import numpy as np
+    span = int(half * 28.5) + 10**6
+    p = ctx.primes_range(10**12 - span, 10**12)[-half:]
+    rng = np.random.default_rng(seed)
+    r = rng.integers(0, 2**63, size=half, dtype=np.uint64) * 2 + 1
+    n = np.concatenate([p, r])
+    perm = rng.permutation(n.size)
+    return n[perm], perm < p.size
+
+
+def run_mr(a) -> None:
+    """Batched verification: 1e8 candidates through deterministic Miller-Rabin (12 bases), and
+    the interior-composite proof of every gap >= 200 below 1e12."""
+    import numpy as np
+    import torch
+    import voss
+    import oracle_lib as O
+    ctx = voss.Context(10**12 + 1)
+    half = 50_000_000
+    n, known = mr_candidates(ctx, half)
+    d_n = torch.from_numpy(n.view(np.int64)).cuda()
+    d_out = torch.empty(n.size, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()  # a real stream handle: 0 would select the context's own stream
+    torch.cuda.synchronize()
+    for _ in range(a.warmup):
+        ctx.mr_verify_device(d_n.data_ptr(), n.size, d_out.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    for e0, e1 in ev:
+        e0.record(stream)
+        ctx.mr_verify_device(d_n.data_ptr(), n.size, d_out.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+    got = d_out.cpu().numpy()
+    # e2e through the host-buffer entry point
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        host = ctx.mr_verify(n)
+    e2e = (time.perf_counter() - t0) / a.steps
+    same_host = bool(np.array_equal(host, got))
+    # CPU baseline: the reference verifier's is_prime_u64 (compiled unmodified) on a sample
+    import os as _os
+    sample = n[: 2_000_000]
+    use_ref = _os.path.exists(O.REF_VERIFY_SO)
+    thr = O.ref_verify().ref_max_threads() if use_ref else O.oracle().oracle_max_threads()
+    t0 = time.perf_counter()
+    ref = O.ref_mr_batch(sample) if use_ref else O.mr_batch(sample)
+    cpu_s = time.perf_counter() - t0
+    match = bool(np.array_equal(ref, got[: sample.size]))
+    # gap proofs: every gap >= 200 below 1e12
+    gaps = ctx.gaps_at_least(1, 10**12 + 1, 200)
+    p_after = gaps["position"].astype(np.uint64)
+    g = gaps["gap"].astype(np.int32)
+    ctx.prove_gaps(p_after[:1000], g[:1000])
+    t0 = time.perf_counter()
+    ok = ctx.prove_gaps(p_after, g)
+    prove_s = time.perf_counter() - t0
+    ps = np.arange(0, p_after.size, max(1, p_after.size // 20000))[:20000]
+    t0 = time.perf_counter()
+    ref_ok = O.ref_prove_gaps(p_after[ps], g[ps]) if use_ref else O.prove_gaps(p_after[ps], g[ps])
+    cpu_prove_s = time.perf_counter() - t0
+    out = {
+        "metric": "Miller-Rabin candidates/s (1e8 candidates: 5e7 primes below 1e12 + 5e7 random odd u64)",
+        "value": n.size / (ms * 1e-3), "unit": "candidates/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic: sieved primes + PCG64 seed 20261203 odd values",
+        "config": {"workload": "batched Miller-Rabin, bases 2..37, 64-bit Montgomery", "candidates": int(n.size),
+                   "known_primes": int(known.sum())},
+        "e2e": {"value": n.size / e2e, "unit": "candidates/s", "h2d_bytes_per_step": 8 * int(n.size),
+                "d2h_bytes_per_step": int(n.size), "api": "voss_mr_verify (host buffers)"},
+        "primes_found": int(got.sum()), "known_primes_all_prime": bool(got[known].all()),
+        "host_equals_device": same_host,
+        "cpu_baseline": {"value": sample.size / cpu_s, "unit": "candidates/s", "cores": thr,
+                         "kind": "reference" if use_ref else "port",
+                         "sample": f"first {sample.size} candidates through verify_cpp.cpp is_prime_u64",
+                         "matches_gpu": match},
+        "gap_proofs": {"gaps_ge_200_below_1e12": int(p_after.size), "all_verified": bool(ok.all()),
+                       "gpu_s": prove_s, "gpu_gaps_per_s": p_after.size / prove_s,
+                       "cpu_reference_gaps_per_s": ps.size / cpu_prove_s, "cpu_cores": thr,
+                       "cpu_sample": int(ps.size), "cpu_matches_gpu": bool(np.array_equal(ref_ok, ok[ps]))},
     }
     print(json.dumps(out), flush=True)
 
@@ -282,6 +370,9 @@ def main():
         return
     if a.workload == "intervals":
         run_intervals(a)
+        return
+    if a.workload == "mr":
+        run_mr(a)
         return
     import numpy as np
     import torch

@@ -165,6 +165,14 @@ VOSS_API int voss_fetch_range(voss_ctx* ctx, voss_range_stats* stats, voss_large
 VOSS_API int voss_primes_range(voss_ctx* ctx, uint64_t lo, uint64_t hi, uint64_t* out,
                                uint64_t cap, uint64_t* count);
 
+/* Every gap g >= min_gap (min_gap >= 3) between consecutive primes of [lo, hi), as
+ * (p_after, g, merit = g / log(p_before)) in ascending position order: the input list of the
+ * interior-composite proofs.  *count receives the number found; out holds min(count, cap).
+ * The reference's large-gap rule is fixed (gap >= 500 or merit >= 10, src/voss_v7_live.cu:291);
+ * this entry point has no counterpart there. */
+VOSS_API int voss_gaps_at_least(voss_ctx* ctx, uint64_t lo, uint64_t hi, uint32_t min_gap,
+                                voss_large_gap* out, uint64_t cap, uint64_t* count);
+
 /* ---- batched intervals ----------------------------------------------------- */
 /* Sieve n independent intervals [lo[i], hi[i]) in one persistent launch over an
  * (interval, tile) work queue and fill out[i].  The reference has no interval API; each

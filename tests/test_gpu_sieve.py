@@ -150,3 +150,15 @@ def test_interval_near_1e18(gpu_ctx_big):
     g = gpu_ctx_big.sieve_range(lo, hi)
     o = O.sieve_range(lo, hi)
     assert_range_equal(g, o)
+
+
+def test_gaps_at_least_matches_oracle(gpu_ctx):
+    for lo, hi, gmin in [(1, 10**7, 100), (10**9, 10**9 + 5 * 10**7, 150), (10**12 - 10**8, 10**12, 200)]:
+        ps = O.primes_range(lo, hi).astype(np.int64)
+        d = np.diff(ps)
+        sel = np.nonzero(d >= gmin)[0]
+        got = gpu_ctx.gaps_at_least(lo, hi, gmin)
+        np.testing.assert_array_equal(got["position"], ps[sel + 1].astype(np.uint64))
+        np.testing.assert_array_equal(got["gap"], d[sel].astype(np.int32))
+        want_m = (d[sel] / np.log(ps[sel].astype(np.float64))).astype(np.float32)
+        np.testing.assert_allclose(got["merit"], want_m, rtol=4e-6)

@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdint>
 
+#include "voss.h"
 #include "voss_internal.h"
 
 namespace voss {
@@ -613,10 +614,11 @@ sieve_tiles_kernel(SieveArgs a) {
             mg = g;
             mlo = (uint32_t)prev;
           }
-          if (a.want_large && g > 100u && !crossing && (g >= 500u || g >= gthr)) {
+          const bool cand = a.large_min_gap ? (g >= a.large_min_gap) : (g > 100u && (g >= 500u || g >= gthr));
+          if (a.want_large && cand && !crossing) {
             const uint64_t v0 = H.vbase + (uint32_t)prev;
             const double merit_d = (double)g / log((double)v0);
-            if (g >= 500u || merit_d >= 10.0) {
+            if (a.large_min_gap || g >= 500u || merit_d >= 10.0) {
               const uint32_t slot = atomicAdd(a.large_count, 1u);
               if (slot < a.large_cap) {
                 a.large[slot] = LargeGapDev{H.vbase + pos, (int32_t)g, (float)merit_d};
@@ -699,9 +701,10 @@ __global__ void stitch_kernel(SieveArgs a) {
   }
   a.partials[t].bgap = (uint32_t)(g > 0xFFFFFFFFull ? 0xFFFFFFFFull : g);
   a.partials[t].bgap_lo = lo_p;
-  if (a.want_large && g > 100 && !crossing) {
+  const bool cand = a.large_min_gap ? (g >= a.large_min_gap) : (g > 100);
+  if (a.want_large && cand && !crossing) {
     const double merit_d = (double)g / log((double)lo_p);
-    if (g >= 500 || merit_d >= 10.0) {
+    if (a.large_min_gap || g >= 500 || merit_d >= 10.0) {
       const uint32_t slot = atomicAdd(a.large_count, 1u);
       if (slot < a.large_cap) {
         a.large[slot] = LargeGapDev{hi_p, (int32_t)g, (float)merit_d};
@@ -764,6 +767,41 @@ __global__ void reduce_kernel(SieveArgs a, IntervalOut* out) {
     o.max_gap_lo = G ? s_lo : 0;
     out[ivx] = o;
   }
+}
+
+// One block per interval: fold the accumulators into voss_interval_stats on the device, so
+// that only the result (not the raw counters) crosses to the host.  lo/hi and the primes
+// 2, 3, 5 are filled in on the host.
+__global__ void interval_finalize_kernel(SieveArgs a, const IntervalOut* io, voss_interval_stats* out) {
+  const uint32_t ivx = blockIdx.x;
+  if (ivx >= a.n_intervals) return;
+  const unsigned long long* A = a.acc + (size_t)ivx * kAccStride;
+  voss_interval_stats* s = out + ivx;
+  for (uint32_t b = threadIdx.x; b < (uint32_t)VOSS_IHIST; b += blockDim.x) {
+    unsigned long long v = 0;
+    if (b > 0) {
+      v = A[kAccHist + b];
+      if (b < (uint32_t)kModqBins)
+        for (uint32_t o = 0; o < 8; ++o) v += A[kAccModq + o * kModqBins + b];
+    }
+    s->gap_hist[b] = v;
+  }
+  if (threadIdx.x == 0) {
+    s->lo = 0;
+    s->hi = 0;
+    s->prime_count = A[kAccCount];
+    s->first_prime = io[ivx].first;
+    s->last_prime = io[ivx].last;
+    s->max_gap = io[ivx].max_gap;
+    s->max_gap_lo = io[ivx].max_gap_lo;
+    s->gap_overflow = A[kAccHistOver];
+  }
+}
+
+int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_interval_stats* out, void* stream) {
+  if (a.n_intervals == 0) return 0;
+  interval_finalize_kernel<<<a.n_intervals, 256, 0, (cudaStream_t)stream>>>(a, io, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 // ---- shared-memory RMW probe ------------------------------------------------------------

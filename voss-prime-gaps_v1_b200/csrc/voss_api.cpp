@@ -119,7 +119,7 @@ std::vector<uint32_t> base_primes(uint64_t limit) {
 }
 
 struct Workspace {
-  DevBuf iv, partials, acc, out, large, large_iv, over, counters, istats, offsets, emit, mr_work;
+  DevBuf iv, partials, acc, out, large, large_iv, over, counters, istats, offsets, emit, mr_work, mr_in, mr_out;
 };
 
 }  // namespace
@@ -213,7 +213,7 @@ int plan_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, ui
 enum { kCtrTile = 0, kCtrLarge = 1, kCtrOver = 2, kCtrError = 3, kCtrMrWork = 4, kCtrWords = 8 };
 
 int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_cap, bool emit,
-                cudaStream_t s) {
+                cudaStream_t s, uint32_t min_gap = 0, SieveArgs* args_out = nullptr) {
   Workspace& W = c->ws;
   const uint32_t n_iv = (uint32_t)P.iv.size();
   int rc;
@@ -244,6 +244,7 @@ int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_c
   a.coop_div = c->tune.coop_div;
   a.mult_factor = c->tune.mult_factor;
   a.want_large = want_large ? 1u : 0u;
+  a.large_min_gap = min_gap;
   a.b_mode = c->tune.medium_mode;
   uint32_t* ctr = W.counters.as<uint32_t>();
   a.tile_counter = ctr + kCtrTile;
@@ -278,6 +279,7 @@ int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_c
     if (launch_reduce(a, W.out.as<IntervalOut>(), s)) return fail(VOSS_ERR_CUDA, "reduce launch failed");
   }
   CUDA_TRY(cudaEventRecord(c->ev2, s));
+  if (args_out) *args_out = a;
   return VOSS_OK;
 }
 
@@ -631,55 +633,72 @@ VOSS_API int voss_sieve_intervals(voss_ctx* c, const uint64_t* lo, const uint64_
   RunPlan P;
   int rc = plan_intervals(c, lo, hi, n, 0, &P);
   if (rc) return rc;
-  rc = launch_plan(c, P, false, 0, false, c->stream);
+  SieveArgs a;
+  rc = launch_plan(c, P, false, 0, false, c->stream, 0, &a);
   if (rc) return rc;
-  std::vector<unsigned long long> acc;
-  std::vector<IntervalOut> outs;
-  std::vector<OverflowGap> over;
+  if ((rc = c->ws.istats.ensure(sizeof(voss_interval_stats) * n))) return rc;
+  if (launch_interval_finalize(a, c->ws.out.as<IntervalOut>(), c->ws.istats.as<voss_interval_stats>(), c->stream))
+    return fail(VOSS_ERR_CUDA, "interval finalize launch failed");
   uint32_t ctr[kCtrWords];
-  rc = fetch_common(c, n, acc, outs, ctr, over, true);
-  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(out, c->ws.istats.p, sizeof(voss_interval_stats) * n, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if ((rc = check_device_error(c, ctr))) return rc;
   cudaEventElapsedTime(&c->sieve_ms, c->ev0, c->ev1);
   cudaEventElapsedTime(&c->total_ms, c->ev0, c->ev2);
   for (uint32_t i = 0; i < n; ++i) {
-    const unsigned long long* A = acc.data() + (size_t)i * kAccStride;
-    voss_interval_stats& s = out[i];
-    std::memset(&s, 0, sizeof(s));
-    s.lo = lo[i];
-    s.hi = hi[i];
-    s.prime_count = A[kAccCount];
-    for (int b = 1; b < kHistBins; ++b) {
-      uint64_t v = A[kAccHist + b];
-      if (b < kModqBins)
-        for (int r = 0; r < 8; ++r) v += A[kAccModq + r * kModqBins + b];
-      s.gap_hist[b] = v;
-    }
-    s.gap_overflow = A[kAccHistOver];
-    s.first_prime = outs[i].first;
-    s.last_prime = outs[i].last;
-    s.max_gap = outs[i].max_gap;
-    s.max_gap_lo = outs[i].max_gap_lo;
+    voss_interval_stats& st = out[i];
+    st.lo = lo[i];
+    st.hi = hi[i];
     const std::vector<uint64_t> sp = small_primes_in(lo[i], hi[i]);
-    if (!sp.empty()) {
-      std::vector<uint64_t> seq = sp;
-      if (outs[i].first) seq.push_back(outs[i].first);
-      uint64_t sm_max = 0, sm_lo = 0;
-      for (size_t k = 1; k < seq.size(); ++k) {
-        const uint64_t g = seq[k] - seq[k - 1];
-        s.gap_hist[g >> 1]++;
-        if (g > sm_max) {
-          sm_max = g;
-          sm_lo = seq[k - 1];
-        }
+    if (sp.empty()) continue;
+    std::vector<uint64_t> seq = sp;
+    if (st.first_prime) seq.push_back(st.first_prime);
+    uint64_t sm_max = 0, sm_lo = 0;
+    for (size_t k = 1; k < seq.size(); ++k) {
+      const uint64_t g = seq[k] - seq[k - 1];
+      st.gap_hist[g >> 1]++;
+      if (g > sm_max) {
+        sm_max = g;
+        sm_lo = seq[k - 1];
       }
-      if (sm_max >= s.max_gap) {
-        s.max_gap = sm_max;
-        s.max_gap_lo = sm_lo;
-      }
-      s.prime_count += sp.size();
-      s.first_prime = sp.front();
-      if (!outs[i].last) s.last_prime = sp.back();
     }
+    if (sm_max >= st.max_gap) {  // earlier pairs win ties
+      st.max_gap = sm_max;
+      st.max_gap_lo = sm_lo;
+    }
+    st.prime_count += sp.size();
+    if (!st.last_prime) st.last_prime = sp.back();
+    st.first_prime = sp.front();
+  }
+  return VOSS_OK;
+}
+
+VOSS_API int voss_gaps_at_least(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t min_gap, voss_large_gap* out,
+                                uint64_t cap, uint64_t* count) {
+  if (!c || !count || (cap && !out)) return fail(VOSS_ERR_ARG, "NULL argument");
+  if (min_gap < 3) return fail(VOSS_ERR_ARG, "min_gap must be at least 3");
+  if (hi < lo) return fail(VOSS_ERR_ARG, "hi < lo");
+  if (hi > c->max_hi) return fail(VOSS_ERR_RANGE, "hi exceeds the context limit");
+  cudaSetDevice(c->device);
+  RunPlan P;
+  int rc = plan_intervals(c, &lo, &hi, 1, 0, &P);
+  if (rc) return rc;
+  const uint64_t devcap = std::min<uint64_t>(std::max<uint64_t>(cap, 1), kMaxLargeCap);
+  rc = launch_plan(c, P, true, devcap, false, c->stream, min_gap);
+  if (rc) return rc;
+  uint32_t ctr[kCtrWords];
+  CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if ((rc = check_device_error(c, ctr))) return rc;
+  const uint64_t found = ctr[kCtrLarge];
+  *count = found;
+  const uint64_t w = std::min<uint64_t>(std::min<uint64_t>(found, devcap), cap);
+  if (w) {
+    std::vector<voss_large_gap> v(std::min<uint64_t>(found, devcap));
+    CUDA_TRY(cudaMemcpy(v.data(), c->ws.large.p, sizeof(voss_large_gap) * v.size(), cudaMemcpyDeviceToHost));
+    std::sort(v.begin(), v.end(), [](const voss_large_gap& x, const voss_large_gap& y) { return x.position < y.position; });
+    std::memcpy(out, v.data(), sizeof(voss_large_gap) * w);
   }
   return VOSS_OK;
 }
@@ -750,14 +769,15 @@ VOSS_API int voss_mr_verify(voss_ctx* c, const uint64_t* n, uint64_t count, uint
   if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
   if (count == 0) return VOSS_OK;
   if (!n || !is_prime) return fail(VOSS_ERR_ARG, "NULL argument");
+  if (count > 0xFFFFFFFFull) return fail(VOSS_ERR_ARG, "count must be < 2^32 per call");
   cudaSetDevice(c->device);
   cudaStream_t s = c->stream;
-  DevBuf dn, dout;
   int rc;
-  if ((rc = dn.ensure(count * 8)) || (rc = dout.ensure(count))) return rc;
-  CUDA_TRY(cudaMemcpyAsync(dn.p, n, count * 8, cudaMemcpyHostToDevice, s));
-  if ((rc = voss_mr_verify_device(c, dn.as<uint64_t>(), count, dout.as<uint8_t>(), s))) return rc;
-  CUDA_TRY(cudaMemcpyAsync(is_prime, dout.p, count, cudaMemcpyDeviceToHost, s));
+  // context-owned, grow-only buffers: repeated calls do not allocate
+  if ((rc = c->ws.mr_in.ensure(count * 8)) || (rc = c->ws.mr_out.ensure(count))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(c->ws.mr_in.p, n, count * 8, cudaMemcpyHostToDevice, s));
+  if ((rc = voss_mr_verify_device(c, c->ws.mr_in.as<uint64_t>(), count, c->ws.mr_out.as<uint8_t>(), s))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(is_prime, c->ws.mr_out.p, count, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   return VOSS_OK;
 }

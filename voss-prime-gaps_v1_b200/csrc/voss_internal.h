@@ -107,6 +107,7 @@ struct SieveArgs {
   uint32_t coop_div;
   uint32_t mult_factor;
   uint32_t want_large;      // record large gaps
+  uint32_t large_min_gap;   // 0: the reference's rule (gap >= 500 or merit >= 10); else every gap >= it
   uint32_t b_mode;          // medium primes: 0 = thread per prime, 1 = lane per (prime, residue)
   uint32_t* tile_counter;
   TilePartial* partials;
@@ -136,6 +137,10 @@ int launch_sieve_stats(const SieveArgs& a, int grid, int block, size_t smem, voi
 int launch_sieve_emit(const SieveArgs& a, int grid, int block, size_t smem, void* stream);
 int launch_stitch(const SieveArgs& a, void* stream);
 int launch_reduce(const SieveArgs& a, IntervalOut* out, void* stream);
+}  // namespace voss
+struct voss_interval_stats;
+namespace voss {
+int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_interval_stats* out, void* stream);
 int sieve_kernel_attrs(int block, size_t smem, int* max_ctas_per_sm);
 void build_presieve_tables(uint32_t* out /* kPreWords */);
 int probe_smem_rmw(int sm_count, void* stream, float* ms, double* bytes);

@@ -80,6 +80,8 @@ SIGNATURES = {
                                  POINTER(LargeGap), c_uint64, POINTER(c_uint64)]),
     "voss_sieve_range_device": (c_int, [c_void_p, c_uint64, c_uint64, c_uint32, c_uint64, c_void_p]),
     "voss_fetch_range": (c_int, [c_void_p, POINTER(RangeStats), POINTER(LargeGap), c_uint64, POINTER(c_uint64)]),
+    "voss_gaps_at_least": (c_int, [c_void_p, c_uint64, c_uint64, c_uint32, POINTER(LargeGap), c_uint64,
+                                   POINTER(c_uint64)]),
     "voss_primes_range": (c_int, [c_void_p, c_uint64, c_uint64, POINTER(c_uint64), c_uint64, POINTER(c_uint64)]),
     "voss_sieve_intervals": (c_int, [c_void_p, POINTER(c_uint64), POINTER(c_uint64), c_uint32,
                                      POINTER(IntervalStats)]),

@@ -159,6 +159,19 @@ class Context:
         N.check(self.lib.voss_primes_range(self._h, lo, hi, _u64p(out), cap, byref(cnt)))
         return out[: min(cap, cnt.value)]
 
+    def gaps_at_least(self, lo: int, hi: int, min_gap: int, cap: int | None = None) -> np.ndarray:
+        """All gaps >= min_gap in [lo, hi) as LARGE_DTYPE records (position = upper prime)."""
+        cnt = c_uint64()
+        if cap is None:
+            cap = 1 << 20
+        while True:
+            out = np.zeros(max(cap, 1), dtype=LARGE_DTYPE)
+            N.check(self.lib.voss_gaps_at_least(self._h, lo, hi, min_gap,
+                                                out.ctypes.data_as(ctypes.POINTER(N.LargeGap)), cap, byref(cnt)))
+            if cnt.value <= cap:
+                return out[: cnt.value]
+            cap = cnt.value
+
     def sieve_intervals(self, lo, hi) -> np.ndarray:
         lo = np.ascontiguousarray(lo, dtype=np.uint64)
         hi = np.ascontiguousarray(hi, dtype=np.uint64)

@@ -223,6 +223,50 @@ VOSS_API int voss_stats_merge(const voss_range_stats* parts, uint32_t n, voss_ra
                               voss_large_gap* large, uint64_t n_large, uint64_t large_cap,
                               uint64_t* large_written);
 
+/* ---- serving: continuous batching ------------------------------------------------ */
+/* A request server over one context.  Client threads submit interval-sieve + gap-statistics
+ * requests and Miller-Rabin batches; a scheduler thread launches the pending requests, in
+ * arrival order, as one batch on whichever of `slots` streams is free (one persistent tile
+ * launch for all the batch's intervals, one Miller-Rabin launch for all its candidates), so
+ * requests that arrive while others run are admitted as slots free up and batches overlap on
+ * the device.  Each slot's device memory and pinned staging is sized at creation from the
+ * config (requests, tiles = bitmap memory, candidates); serving then allocates nothing on the
+ * device.  Every wait is bounded.  The server is thread-safe; while it runs, the context's own
+ * entry points may be used only from one other thread.  No counterpart in the reference. */
+typedef struct voss_server voss_server;
+typedef struct voss_server_config {
+  uint32_t slots;                 /* batches in flight (streams); default 4 */
+  uint32_t max_batch_requests;    /* interval requests per batch; default 1024 */
+  uint32_t max_batch_tiles;       /* tiles per batch (one tile = 6.02e6 integers by default); default 65536 */
+  uint32_t fail_every_n_batches;  /* testing: fail every n-th batch on the host (0 = never) */
+  uint64_t max_batch_candidates;  /* Miller-Rabin candidates per batch; default 1 << 22 */
+  uint64_t reserved[2];
+} voss_server_config;
+typedef struct voss_server_stats {
+  uint64_t batches, completed, failed, pending, kernel_launches;
+  uint32_t max_inflight_batches;
+  uint32_t reserved0;
+  double mean_batch_requests;
+} voss_server_stats;
+
+VOSS_API int voss_server_create(voss_ctx* ctx, const voss_server_config* cfg, voss_server** out);
+/* Drains queued and running requests, then stops the scheduler and frees the slots. */
+VOSS_API void voss_server_destroy(voss_server* srv);
+/* Queue [lo, hi); the answer is a voss_interval_stats equal to voss_sieve_intervals on it alone. */
+VOSS_API int voss_server_submit_interval(voss_server* srv, uint64_t lo, uint64_t hi, uint64_t* ticket);
+/* Queue Miller-Rabin verdicts for n[0..count) (copied at submission). */
+VOSS_API int voss_server_submit_mr(voss_server* srv, const uint64_t* n, uint64_t count, uint64_t* ticket);
+/* VOSS_OK once the request finished, VOSS_ERR_TIMEOUT after timeout_ms, or the request's error. */
+VOSS_API int voss_server_wait(voss_server* srv, uint64_t ticket, uint32_t timeout_ms);
+VOSS_API int voss_server_result_interval(voss_server* srv, uint64_t ticket, voss_interval_stats* out);
+VOSS_API int voss_server_result_mr(voss_server* srv, uint64_t ticket, uint8_t* out, uint64_t count);
+/* Seconds since server creation at submission, batch start and completion (-1 if not yet). */
+VOSS_API int voss_server_request_times(voss_server* srv, uint64_t ticket, double* submit_s, double* start_s,
+                                       double* done_s);
+/* Forget a finished request (voss_request_free). */
+VOSS_API int voss_server_release(voss_server* srv, uint64_t ticket);
+VOSS_API int voss_server_get_stats(voss_server* srv, voss_server_stats* out);
+
 /* ---- diagnostics --------------------------------------------------------------- */
 /* Shared-memory read-modify-write bandwidth of this device (GB/s, 8 bytes per 32-bit
  * atomicAnd), measured by a bank-conflict-free kernel: the roofline denominator of the

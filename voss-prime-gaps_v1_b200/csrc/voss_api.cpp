@@ -18,10 +18,11 @@
 
 #include "voss.h"
 #include "voss_internal.h"
+#include "voss_host.h"
 
 using namespace voss;
 
-namespace {
+namespace voss_host {
 
 thread_local std::string g_err;
 
@@ -35,45 +36,23 @@ int fail(int code, const char* fmt, ...) {
   return code;
 }
 
-#define CUDA_TRY(call)                                                                   \
-  do {                                                                                   \
-    cudaError_t e__ = (call);                                                            \
-    if (e__ != cudaSuccess)                                                              \
-      return fail(VOSS_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e__));      \
-  } while (0)
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-  int ensure(size_t need) {
-    if (need <= bytes) return VOSS_OK;
-    if (p) cudaFree(p);
+int DevBuf::ensure(size_t need) {
+  if (need <= bytes) return VOSS_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+  size_t n = need < 256 ? 256 : need + need / 4;
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
     p = nullptr;
-    bytes = 0;
-    size_t n = need < 256 ? 256 : need + need / 4;
-    cudaError_t e = cudaMalloc(&p, n);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      return fail(VOSS_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", n, cudaGetErrorString(e));
-    }
-    bytes = n;
-    return VOSS_OK;
+    return fail(VOSS_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", n, cudaGetErrorString(e));
   }
-  template <class T>
-  T* as() const {
-    return static_cast<T*>(p);
-  }
-};
+  bytes = n;
+  return VOSS_OK;
+}
 
 const int kW30[8] = {1, 7, 11, 13, 17, 19, 23, 29};
 const int kQ[VOSS_NUM_Q] = VOSS_Q_LIST;
-constexpr uint64_t kMaxHi = 1ull << 62;
-constexpr uint32_t kOverCap = 1u << 16;
-constexpr uint64_t kDefaultLargeCap = 1ull << 22;
-constexpr uint64_t kMaxLargeCap = 50000000ull;  // MAX_LARGE_GAPS, src/voss_v7_live.cu:34
 
 uint64_t isqrt_u64(uint64_t x) {
   uint64_t s = (uint64_t)std::sqrt((long double)x);
@@ -118,37 +97,15 @@ std::vector<uint32_t> base_primes(uint64_t limit) {
   return out;
 }
 
-struct Workspace {
-  DevBuf iv, partials, acc, out, large, large_iv, over, counters, istats, offsets, emit, mr_work, mr_in, mr_out;
-};
 
 }  // namespace
 
 namespace voss_detail {
-int set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+int set_error(int code, const char* msg) { return voss_host::fail(code, "%s", msg); }
 }  // namespace voss_detail
 
-struct voss_ctx {
-  int device = 0;
-  int sm_count = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
-  uint64_t max_hi = 0;
-  std::vector<uint32_t> primes;  // >= 37
-  DevBuf d_primes, d_magic, d_pretab;
-  voss_tuning tune{};
-  int ctas_per_sm = 1;
-  Workspace ws;
-  // last range run
-  bool have_range = false;
-  uint64_t r_lo = 0, r_hi = 0, r_seg = 0;
-  uint32_t r_flags = 0;
-  uint32_t r_tiles = 0;
-  uint64_t r_large_cap = 0;
-  float sieve_ms = 0, total_ms = 0;
-};
 
-namespace {
+namespace voss_host {
 
 int apply_tuning(voss_ctx* c, const voss_tuning& t0) {
   voss_tuning t = t0;
@@ -173,10 +130,6 @@ int apply_tuning(voss_ctx* c, const voss_tuning& t0) {
   return VOSS_OK;
 }
 
-struct RunPlan {
-  std::vector<IntervalDev> iv;
-  uint32_t n_tiles = 0;
-};
 
 // Cut intervals [lo_i, hi_i) into tiles; intervals without wheel integers get no tiles.
 int plan_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, uint32_t n,
@@ -210,11 +163,9 @@ int plan_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, ui
   return VOSS_OK;
 }
 
-enum { kCtrTile = 0, kCtrLarge = 1, kCtrOver = 2, kCtrError = 3, kCtrMrWork = 4, kCtrWords = 8 };
 
-int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_cap, bool emit,
-                cudaStream_t s, uint32_t min_gap = 0, SieveArgs* args_out = nullptr) {
-  Workspace& W = c->ws;
+int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPlan& P, bool want_large,
+                   uint64_t large_cap, bool emit, cudaStream_t s, uint32_t min_gap, SieveArgs* args_out) {
   const uint32_t n_iv = (uint32_t)P.iv.size();
   int rc;
   if ((rc = W.iv.ensure(sizeof(IntervalDev) * std::max<size_t>(1, n_iv)))) return rc;
@@ -267,27 +218,35 @@ int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_c
   const size_t smem = sieve_smem_bytes(tw);
   const int slots = c->sm_count * c->ctas_per_sm;
   const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(P.n_tiles, (uint32_t)slots));
-  CUDA_TRY(cudaEventRecord(c->ev0, s));
+  CUDA_TRY(cudaEventRecord(E.ev0, s));
   if (P.n_tiles) {
     int lr = emit ? launch_sieve_emit(a, grid, (int)c->tune.block_threads, smem, s)
                   : launch_sieve_stats(a, grid, (int)c->tune.block_threads, smem, s);
     if (lr) return fail(VOSS_ERR_CUDA, "sieve launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
-  CUDA_TRY(cudaEventRecord(c->ev1, s));
+  CUDA_TRY(cudaEventRecord(E.ev1, s));
   if (!emit) {
     if (launch_stitch(a, s)) return fail(VOSS_ERR_CUDA, "stitch launch failed");
     if (launch_reduce(a, W.out.as<IntervalOut>(), s)) return fail(VOSS_ERR_CUDA, "reduce launch failed");
   }
-  CUDA_TRY(cudaEventRecord(c->ev2, s));
+  CUDA_TRY(cudaEventRecord(E.ev2, s));
   if (args_out) *args_out = a;
   return VOSS_OK;
 }
 
-int check_device_error(voss_ctx* c, uint32_t* ctr_host) {
+int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_cap, bool emit, cudaStream_t s,
+                uint32_t min_gap = 0, SieveArgs* args_out = nullptr) {
+  LaunchEvents E;
+  E.ev0 = c->ev0;
+  E.ev1 = c->ev1;
+  E.ev2 = c->ev2;
+  return launch_plan_ws(c, c->ws, E, P, want_large, large_cap, emit, s, min_gap, args_out);
+}
+
+int check_device_error(const uint32_t* ctr_host) {
   if (ctr_host[kCtrError] & kErrBounds) return fail(VOSS_ERR_DEVICE, "kernel bounds check failed");
   if (ctr_host[kCtrError] & kErrOverflowList) return fail(VOSS_ERR_DEVICE, "gap overflow list full");
   if (ctr_host[kCtrError]) return fail(VOSS_ERR_DEVICE, "kernel error word 0x%x", ctr_host[kCtrError]);
-  (void)c;
   return VOSS_OK;
 }
 
@@ -297,6 +256,31 @@ std::vector<uint64_t> small_primes_in(uint64_t lo, uint64_t hi) {
   for (uint64_t p : {2ull, 3ull, 5ull})
     if (p >= lo && p < hi) v.push_back(p);
   return v;
+}
+
+void add_small_primes(voss_interval_stats& st, uint64_t lo, uint64_t hi) {
+  st.lo = lo;
+  st.hi = hi;
+  const std::vector<uint64_t> sp = small_primes_in(lo, hi);
+  if (sp.empty()) return;
+  std::vector<uint64_t> seq = sp;
+  if (st.first_prime) seq.push_back(st.first_prime);
+  uint64_t sm_max = 0, sm_lo = 0;
+  for (size_t k = 1; k < seq.size(); ++k) {
+    const uint64_t g = seq[k] - seq[k - 1];
+    st.gap_hist[g >> 1]++;
+    if (g > sm_max) {
+      sm_max = g;
+      sm_lo = seq[k - 1];
+    }
+  }
+  if (sm_max >= st.max_gap) {  // earlier pairs win ties
+    st.max_gap = sm_max;
+    st.max_gap_lo = sm_lo;
+  }
+  st.prime_count += sp.size();
+  if (!st.last_prime) st.last_prime = sp.back();
+  st.first_prime = sp.front();
 }
 
 int row30(uint64_t p) {
@@ -410,7 +394,7 @@ int fetch_common(voss_ctx* c, uint32_t n_iv, std::vector<unsigned long long>& ac
                              cudaMemcpyDeviceToHost, s));
   }
   CUDA_TRY(cudaStreamSynchronize(s));
-  int rc = check_device_error(c, ctr);
+  int rc = check_device_error(ctr);
   if (rc) return rc;
   const uint32_t no = std::min(ctr[kCtrOver], kOverCap);
   over.resize(no);
@@ -478,6 +462,8 @@ int fetch_range(voss_ctx* c, voss_range_stats* st, voss_large_gap* large, uint64
 // =====================================================================================
 // C ABI
 // =====================================================================================
+using namespace voss_host;
+
 extern "C" {
 
 VOSS_API const char* voss_version(void) { return "voss-b200 0.1 (sm_100a)"; }
@@ -643,34 +629,10 @@ VOSS_API int voss_sieve_intervals(voss_ctx* c, const uint64_t* lo, const uint64_
   CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaMemcpyAsync(out, c->ws.istats.p, sizeof(voss_interval_stats) * n, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
-  if ((rc = check_device_error(c, ctr))) return rc;
+  if ((rc = check_device_error(ctr))) return rc;
   cudaEventElapsedTime(&c->sieve_ms, c->ev0, c->ev1);
   cudaEventElapsedTime(&c->total_ms, c->ev0, c->ev2);
-  for (uint32_t i = 0; i < n; ++i) {
-    voss_interval_stats& st = out[i];
-    st.lo = lo[i];
-    st.hi = hi[i];
-    const std::vector<uint64_t> sp = small_primes_in(lo[i], hi[i]);
-    if (sp.empty()) continue;
-    std::vector<uint64_t> seq = sp;
-    if (st.first_prime) seq.push_back(st.first_prime);
-    uint64_t sm_max = 0, sm_lo = 0;
-    for (size_t k = 1; k < seq.size(); ++k) {
-      const uint64_t g = seq[k] - seq[k - 1];
-      st.gap_hist[g >> 1]++;
-      if (g > sm_max) {
-        sm_max = g;
-        sm_lo = seq[k - 1];
-      }
-    }
-    if (sm_max >= st.max_gap) {  // earlier pairs win ties
-      st.max_gap = sm_max;
-      st.max_gap_lo = sm_lo;
-    }
-    st.prime_count += sp.size();
-    if (!st.last_prime) st.last_prime = sp.back();
-    st.first_prime = sp.front();
-  }
+  for (uint32_t i = 0; i < n; ++i) add_small_primes(out[i], lo[i], hi[i]);
   return VOSS_OK;
 }
 
@@ -690,7 +652,7 @@ VOSS_API int voss_gaps_at_least(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t 
   uint32_t ctr[kCtrWords];
   CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
-  if ((rc = check_device_error(c, ctr))) return rc;
+  if ((rc = check_device_error(ctr))) return rc;
   const uint64_t found = ctr[kCtrLarge];
   *count = found;
   const uint64_t w = std::min<uint64_t>(std::min<uint64_t>(found, devcap), cap);
@@ -722,7 +684,7 @@ VOSS_API int voss_primes_range(voss_ctx* c, uint64_t lo, uint64_t hi, uint64_t* 
   uint32_t ctr[kCtrWords];
   CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
-  if ((rc = check_device_error(c, ctr))) return rc;
+  if ((rc = check_device_error(ctr))) return rc;
   std::vector<unsigned long long> offs(std::max<uint32_t>(1, P.n_tiles));
   uint64_t total = 0;
   for (uint32_t t = 0; t < P.n_tiles; ++t) {
@@ -747,7 +709,7 @@ VOSS_API int voss_primes_range(voss_ctx* c, uint64_t lo, uint64_t hi, uint64_t* 
   CUDA_TRY(cudaMemcpyAsync(out + k, c->ws.emit.p, sizeof(uint64_t) * room, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
-  return check_device_error(c, ctr);
+  return check_device_error(ctr);
 }
 
 VOSS_API int voss_mr_verify_device(voss_ctx* c, const uint64_t* d_n, uint64_t count, uint8_t* d_out,

@@ -1,0 +1,101 @@
+// voss_host.h — host-runtime types shared by the C ABI (voss_api.cpp) and the request server
+// (voss_server.cpp).  Not installed; the public interface is include/voss.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "voss.h"
+#include "voss_internal.h"
+
+namespace voss_host {
+
+// Record a message for voss_last_error() and return `code`.
+int fail(int code, const char* fmt, ...);
+
+#define CUDA_TRY(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e__ = (call);                                                               \
+    if (e__ != cudaSuccess)                                                                 \
+      return ::voss_host::fail(VOSS_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e__)); \
+  } while (0)
+
+// A grow-only device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  int ensure(size_t need);
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// Device memory of one launch of the tile kernel (and of Miller-Rabin batches).
+struct Workspace {
+  DevBuf iv, partials, acc, out, large, large_iv, over, counters, istats, offsets, emit, mr_work, mr_in, mr_out;
+};
+
+// Events bracketing one launch: ev0 before the sieve kernel, ev1 after it, ev2 after the
+// stitch/reduce kernels.
+struct LaunchEvents {
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+};
+
+struct RunPlan {
+  std::vector<voss::IntervalDev> iv;
+  uint32_t n_tiles = 0;
+};
+
+enum { kCtrTile = 0, kCtrLarge = 1, kCtrOver = 2, kCtrError = 3, kCtrMrWork = 4, kCtrWords = 8 };
+
+constexpr uint64_t kMaxHi = 1ull << 62;
+constexpr uint32_t kOverCap = 1u << 16;
+constexpr uint64_t kDefaultLargeCap = 1ull << 22;
+constexpr uint64_t kMaxLargeCap = 50000000ull;  // MAX_LARGE_GAPS, src/voss_v7_live.cu:34
+
+}  // namespace voss_host
+
+struct voss_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  uint64_t max_hi = 0;
+  std::vector<uint32_t> primes;  // >= 37
+  voss_host::DevBuf d_primes, d_magic, d_pretab;
+  voss_tuning tune{};
+  int ctas_per_sm = 1;
+  voss_host::Workspace ws;
+  // last range run
+  bool have_range = false;
+  uint64_t r_lo = 0, r_hi = 0, r_seg = 0;
+  uint32_t r_flags = 0;
+  uint32_t r_tiles = 0;
+  uint64_t r_large_cap = 0;
+  float sieve_ms = 0, total_ms = 0;
+};
+
+namespace voss_host {
+
+// Cut intervals [lo_i, hi_i) into tiles; intervals without wheel integers get no tiles.
+int plan_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, uint32_t n, uint64_t seg_k,
+                   RunPlan* P);
+// Queue the tile kernel (+ stitch and reduce unless emit) for plan P on stream s, using the
+// workspace W and events E.
+int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPlan& P, bool want_large,
+                   uint64_t large_cap, bool emit, cudaStream_t s, uint32_t min_gap, voss::SieveArgs* args_out);
+int check_device_error(const uint32_t* ctr_host);
+std::vector<uint64_t> small_primes_in(uint64_t lo, uint64_t hi);
+// Add the primes 2, 3, 5 of [lo, hi) to a device-finalized interval result.
+void add_small_primes(voss_interval_stats& st, uint64_t lo, uint64_t hi);
+
+}  // namespace voss_host

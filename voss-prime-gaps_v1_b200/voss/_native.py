@@ -66,6 +66,21 @@ class Tuning(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("slots", c_uint32), ("max_batch_requests", c_uint32), ("max_batch_tiles", c_uint32),
+        ("fail_every_n_batches", c_uint32), ("max_batch_candidates", c_uint64), ("reserved", c_uint64 * 2),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("batches", c_uint64), ("completed", c_uint64), ("failed", c_uint64), ("pending", c_uint64),
+        ("kernel_launches", c_uint64), ("max_inflight_batches", c_uint32), ("reserved0", c_uint32),
+        ("mean_batch_requests", c_double),
+    ]
+
+
 # name -> (restype, argtypes); every entry point declared in include/voss.h
 SIGNATURES = {
     "voss_version": (c_char_p, []),
@@ -92,6 +107,16 @@ SIGNATURES = {
     "voss_write_artifacts": (c_int, [POINTER(RangeStats), POINTER(LargeGap), c_uint64, c_char_p]),
     "voss_stats_merge": (c_int, [POINTER(RangeStats), c_uint32, POINTER(RangeStats), POINTER(LargeGap),
                                  c_uint64, c_uint64, POINTER(c_uint64)]),
+    "voss_server_create": (c_int, [c_void_p, POINTER(ServerConfig), POINTER(c_void_p)]),
+    "voss_server_destroy": (None, [c_void_p]),
+    "voss_server_submit_interval": (c_int, [c_void_p, c_uint64, c_uint64, POINTER(c_uint64)]),
+    "voss_server_submit_mr": (c_int, [c_void_p, POINTER(c_uint64), c_uint64, POINTER(c_uint64)]),
+    "voss_server_wait": (c_int, [c_void_p, c_uint64, c_uint32]),
+    "voss_server_result_interval": (c_int, [c_void_p, c_uint64, POINTER(IntervalStats)]),
+    "voss_server_result_mr": (c_int, [c_void_p, c_uint64, POINTER(c_uint8), c_uint64]),
+    "voss_server_request_times": (c_int, [c_void_p, c_uint64, POINTER(c_double), POINTER(c_double), POINTER(c_double)]),
+    "voss_server_release": (c_int, [c_void_p, c_uint64]),
+    "voss_server_get_stats": (c_int, [c_void_p, POINTER(ServerStats)]),
     "voss_probe_smem_rmw": (c_int, [c_void_p, POINTER(c_double)]),
     "voss_last_kernel_ms": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
 }

@@ -240,7 +240,8 @@ typedef struct voss_server_config {
   uint32_t max_batch_tiles;       /* tiles per batch (one tile = 6.02e6 integers by default); default 65536 */
   uint32_t fail_every_n_batches;  /* testing: fail every n-th batch on the host (0 = never) */
   uint64_t max_batch_candidates;  /* Miller-Rabin candidates per batch; default 1 << 22 */
-  uint64_t reserved[2];
+  uint64_t max_batch_bitmap_bytes; /* large-prime bitmap per slot (bytes = integers/30); default 1 GiB */
+  uint64_t reserved[1];
 } voss_server_config;
 typedef struct voss_server_stats {
   uint64_t batches, completed, failed, pending, kernel_launches;

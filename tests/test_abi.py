@@ -47,6 +47,8 @@ int main(void) {
   printf("%zu %zu %zu %zu %zu\n", offsetof(voss_range_stats, mod4), offsetof(voss_range_stats, modq),
          offsetof(voss_range_stats, modq_gap), offsetof(voss_range_stats, large_total), offsetof(voss_range_stats, gap_hist));
   printf("%zu %zu\n", offsetof(voss_interval_stats, gap_overflow), offsetof(voss_interval_stats, gap_hist));
+  printf("%zu %zu %zu %zu\n", sizeof(voss_server_config), offsetof(voss_server_config, max_batch_candidates),
+         sizeof(voss_server_stats), offsetof(voss_server_stats, mean_batch_requests));
   return 0;
 }'''
     with tempfile.TemporaryDirectory() as d:
@@ -59,6 +61,9 @@ int main(void) {
     assert nums[:4] == [ctypes.sizeof(RS), ctypes.sizeof(IS), ctypes.sizeof(N.LargeGap), ctypes.sizeof(N.Tuning)]
     assert nums[4:9] == [RS.mod4.offset, RS.modq.offset, RS.modq_gap.offset, RS.large_total.offset, RS.gap_hist.offset]
     assert nums[9:11] == [IS.gap_overflow.offset, IS.gap_hist.offset]
+    SC, SS = N.ServerConfig, N.ServerStats
+    assert nums[11:15] == [ctypes.sizeof(SC), SC.max_batch_candidates.offset, ctypes.sizeof(SS),
+                           SS.mean_batch_requests.offset]
 
 
 def test_errors_are_returned_not_fatal():

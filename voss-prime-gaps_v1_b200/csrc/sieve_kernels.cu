@@ -38,6 +38,8 @@ __constant__ uint8_t c_wheel_step[64];
 // residue r (mod 30) -> wheel bit index, or -1 when gcd(r, 30) > 1.
 __constant__ int8_t c_res_bit[32];
 
+static int ensure_tables();
+
 // Constant memory is per device: the tables are uploaded once for each device ordinal.
 static std::atomic<uint64_t> g_tables_ready{0};
 
@@ -151,6 +153,7 @@ struct TileHdr {
   uint32_t interval, tile, next_tile, cur_iv, since_flush, flush;
   uint32_t r0, r1;       // base primes lying in the tile (restore)
   uint32_t coop_ctr, b_ctr, c_ctr;  // work counters of the three prime categories
+  unsigned long long gword;         // the tile's first word in the large-prime bitmap
   uint32_t first;
   uint32_t tile_base_rank;
   unsigned long long count_total;
@@ -348,8 +351,10 @@ sieve_tiles_kernel(SieveArgs a) {
       H.lt = 4u * nw;
       uint64_t vend = H.vbase + 30ull * H.lt;
       if (vend > iv.hi) vend = iv.hi;
-      const uint32_t np = count_le(a.primes, a.n_primes, isqrt_u64(vend - 1));
+      uint32_t np = count_le(a.primes, a.n_primes, isqrt_u64(vend - 1));
+      if (a.gbm && np > a.scatter_first) np = a.scatter_first;  // the rest came from the pre-pass
       H.np = np;
+      H.gword = iv.gword + wofs;
       uint32_t ia = count_lt(a.primes, np, (uint64_t)(H.lt / a.coop_div));
       uint32_t ib = count_lt(a.primes, np, (uint64_t)H.lt * a.mult_factor);
       H.ia = ia;
@@ -389,10 +394,12 @@ sieve_tiles_kernel(SieveArgs a) {
         st[g] = (uint32_t)BLOCK % pre_mod(g);
       }
       const uint64_t vbase = H.vbase, vlo = H.vlo, vhi = H.vhi;
+      const uint32_t* gbm = a.gbm ? a.gbm + H.gword : nullptr;
       for (uint32_t w = tid; w < a.tile_words; w += BLOCK) {
         uint32_t m = 0;
         if (w < nw) {
           m = pre[ix[0]] & pre[1001u + ix[1]] & pre[1324u + ix[2]] & pre[1991u + ix[3]];
+          if (gbm) m &= gbm[w];
           const uint64_t v0 = vbase + 120ull * w;
           if (v0 + 1 < vlo || v0 + 120 > vhi) m &= edge_mask(v0, vlo, vhi);
         }
@@ -801,6 +808,55 @@ __global__ void interval_finalize_kernel(SieveArgs a, const IntervalOut* io, vos
 int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_interval_stats* out, void* stream) {
   if (a.n_intervals == 0) return 0;
   interval_finalize_kernel<<<a.n_intervals, 256, 0, (cudaStream_t)stream>>>(a, io, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// Large-prime pre-pass (bucket-free): each thread takes primes p >= 8 * tile bytes in turn and,
+// for every interval of the launch that p can reach (intervals sorted by isqrt(hi - 1),
+// descending, staged in shared memory), walks p's multiples across the interval and clears
+// them in the launch's large-prime bitmap with global atomics.  The prime table is read once
+// per launch instead of once per tile, which is what bounds high intervals (at 1e18 the table
+// is 610 MB).  The tile kernel ANDs this bitmap into its fill and skips these primes.
+constexpr int kScatterChunk = 1024;  // 32 KB of interval descriptors per block
+
+__global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __restrict__ primes,
+                                                            const uint64_t* __restrict__ magic, uint32_t j0,
+                                                            uint32_t j1, const IntervalScatter* __restrict__ iv,
+                                                            uint32_t n_iv, uint32_t* __restrict__ gbm) {
+  __shared__ IntervalScatter s_iv[kScatterChunk];
+  __shared__ int8_t s_rb[32];
+  if (threadIdx.x < 32) s_rb[threadIdx.x] = c_res_bit[threadIdx.x];
+  for (uint32_t i = threadIdx.x; i < n_iv; i += blockDim.x) s_iv[i] = iv[i];
+  __syncthreads();
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t j = j0 + blockIdx.x * blockDim.x + threadIdx.x; j < j1; j += stride) {
+    const uint32_t p = primes[j];
+    const uint64_t m = magic[j];
+    for (uint32_t s = 0; s < n_iv; ++s) {
+      const IntervalScatter I = s_iv[s];
+      if (p > I.sqrt_hi) break;
+      const uint32_t r = mod_barrett(I.vbase, p, m);
+      uint64_t d = r ? (uint64_t)(p - r) : 0ull;
+      for (; d < I.span; d += p) {
+        const uint64_t q = d / 30ull;
+        const int b = s_rb[(uint32_t)(d - 30ull * q)];
+        if (b >= 0) atomicAnd(gbm + I.gword + (q >> 2), ~(1u << ((((uint32_t)q & 3u) << 3) | (uint32_t)b)));
+      }
+    }
+  }
+}
+
+int launch_scatter_large(const uint32_t* primes, const uint64_t* magic, uint32_t j0, uint32_t j1,
+                         const IntervalScatter* iv, uint32_t n_iv, uint32_t* gbm, int sm_count, void* stream) {
+  if (ensure_tables()) return -1;
+  if (j1 <= j0 || n_iv == 0) return 0;
+  const uint32_t per = 512u;
+  const uint64_t want = ((uint64_t)(j1 - j0) + per - 1) / per;
+  const int grid = (int)(want < (uint64_t)sm_count * 4 ? want : (uint64_t)sm_count * 4);
+  for (uint32_t off = 0; off < n_iv; off += kScatterChunk) {
+    const uint32_t n = n_iv - off < (uint32_t)kScatterChunk ? n_iv - off : (uint32_t)kScatterChunk;
+    scatter_large_kernel<<<grid, per, 0, (cudaStream_t)stream>>>(primes, magic, j0, j1, iv + off, n, gbm);
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

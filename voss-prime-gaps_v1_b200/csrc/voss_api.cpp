@@ -136,7 +136,7 @@ int plan_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, ui
                    uint64_t seg_k, RunPlan* P) {
   const uint64_t tw = (uint64_t)c->tune.block_threads * c->tune.chunk_words;
   P->iv.resize(n);
-  uint64_t tiles = 0;
+  uint64_t tiles = 0, words = 0;
   for (uint32_t i = 0; i < n; ++i) {
     IntervalDev& d = P->iv[i];
     std::memset(&d, 0, sizeof(d));
@@ -154,12 +154,15 @@ int plan_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, ui
     const uint64_t kf = a / 30, kl = (hi[i] - 1) / 30;
     d.k0 = kf & ~3ull;
     d.n_words = (kl - d.k0) / 4 + 1;
+    d.gword = words;
+    words += d.n_words;
     const uint64_t nt = (d.n_words + tw - 1) / tw;
     d.n_tiles = (uint32_t)nt;
     tiles += nt;
     if (tiles >= 0x7FFFFFFFull) return fail(VOSS_ERR_RANGE, "too many tiles in one launch; split the range");
   }
   P->n_tiles = (uint32_t)tiles;
+  P->n_words = words;
   return VOSS_OK;
 }
 
@@ -218,7 +221,44 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
   const size_t smem = sieve_smem_bytes(tw);
   const int slots = c->sm_count * c->ctas_per_sm;
   const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(P.n_tiles, (uint32_t)slots));
+  // Large-prime pre-pass: primes p >= mult_factor * tile bytes are applied once per launch
+  // (prime-major) instead of once per tile, when the launch's bitmap fits the budget.
+  const uint64_t p_large = (uint64_t)c->tune.mult_factor * 4ull * tw;
+  uint64_t max_sq = 0;
+  for (const IntervalDev& d : P.iv)
+    if (d.n_tiles) max_sq = std::max<uint64_t>(max_sq, isqrt_u64(d.hi - 1));
+  const uint32_t j0 = (uint32_t)(std::lower_bound(c->primes.begin(), c->primes.end(), p_large) - c->primes.begin());
+  const uint32_t j1 = (uint32_t)(std::upper_bound(c->primes.begin(), c->primes.end(),
+                                                  (uint32_t)std::min<uint64_t>(max_sq, 0xFFFFFFFFull)) -
+                                 c->primes.begin());
+  const size_t gbm_bytes = (size_t)P.n_words * 4;
+  bool scatter = P.n_tiles && j1 > j0 && p_large <= 0xFFFFFFFFull && gbm_bytes <= W.gbm_budget &&
+                 (!W.gbm_fixed || gbm_bytes <= W.gbm.bytes);
+  std::vector<IntervalScatter> sc;
+  if (scatter) {
+    for (const IntervalDev& d : P.iv) {
+      if (!d.n_tiles) continue;
+      const uint64_t sq = isqrt_u64(d.hi - 1);
+      if (sq < p_large) continue;
+      IntervalScatter I;
+      I.vbase = 30ull * d.k0;
+      I.span = 120ull * d.n_words;
+      I.gword = d.gword;
+      I.sqrt_hi = (uint32_t)std::min<uint64_t>(sq, 0xFFFFFFFFull);
+      I.pad = 0;
+      sc.push_back(I);
+    }
+    std::sort(sc.begin(), sc.end(), [](const IntervalScatter& x, const IntervalScatter& y) { return x.sqrt_hi > y.sqrt_hi; });
+    if ((rc = W.gbm.ensure(gbm_bytes)) || (rc = W.scat.ensure(sizeof(IntervalScatter) * sc.size()))) return rc;
+    CUDA_TRY(cudaMemsetAsync(W.gbm.p, 0xFF, gbm_bytes, s));
+    CUDA_TRY(cudaMemcpyAsync(W.scat.p, sc.data(), sizeof(IntervalScatter) * sc.size(), cudaMemcpyHostToDevice, s));
+    a.gbm = W.gbm.as<uint32_t>();
+    a.scatter_first = j0;
+  }
   CUDA_TRY(cudaEventRecord(E.ev0, s));
+  if (scatter && launch_scatter_large(a.primes, a.magic, j0, j1, W.scat.as<IntervalScatter>(), (uint32_t)sc.size(),
+                                      W.gbm.as<uint32_t>(), c->sm_count, s))
+    return fail(VOSS_ERR_CUDA, "large-prime pre-pass launch failed");
   if (P.n_tiles) {
     int lr = emit ? launch_sieve_emit(a, grid, (int)c->tune.block_threads, smem, s)
                   : launch_sieve_stats(a, grid, (int)c->tune.block_threads, smem, s);

@@ -42,6 +42,11 @@ struct DevBuf {
 // Device memory of one launch of the tile kernel (and of Miller-Rabin batches).
 struct Workspace {
   DevBuf iv, partials, acc, out, large, large_iv, over, counters, istats, offsets, emit, mr_work, mr_in, mr_out;
+  DevBuf gbm, scat;  // large-prime pre-pass: bitmap of the launch and its interval descriptors
+  // Largest large-prime bitmap this workspace may use; with gbm_fixed the buffers are never
+  // grown (server slots size them at creation), and launches that need more skip the pre-pass.
+  size_t gbm_budget = 8ull << 30;
+  bool gbm_fixed = false;
 };
 
 // Events bracketing one launch: ev0 before the sieve kernel, ev1 after it, ev2 after the
@@ -53,6 +58,7 @@ struct LaunchEvents {
 struct RunPlan {
   std::vector<voss::IntervalDev> iv;
   uint32_t n_tiles = 0;
+  uint64_t n_words = 0;
 };
 
 enum { kCtrTile = 0, kCtrLarge = 1, kCtrOver = 2, kCtrError = 3, kCtrMrWork = 4, kCtrWords = 8 };

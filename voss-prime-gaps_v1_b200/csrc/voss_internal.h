@@ -65,8 +65,18 @@ struct IntervalDev {
   uint64_t k0;          // first byte of the first tile (multiple of 4)
   uint64_t n_words;     // 32-bit words covering [k0, last byte]
   uint64_t seg_k;       // reference-compat segment length in bytes (0: no segment rule)
+  uint64_t gword;       // first word of the interval in the large-prime bitmap (when used)
   uint32_t tile_begin;  // global index of the interval's first tile
   uint32_t n_tiles;
+};
+
+// One interval as seen by the large-prime pre-pass (sorted by sqrt_hi, descending).
+struct IntervalScatter {
+  uint64_t vbase;    // 30 * k0: the integer at bit 0 of the interval's first word
+  uint64_t span;     // integers covered by the interval's words (120 per word)
+  uint64_t gword;    // first word in the large-prime bitmap
+  uint32_t sqrt_hi;  // isqrt(hi - 1), capped to 2^32 - 1
+  uint32_t pad;
 };
 
 struct TilePartial {
@@ -109,6 +119,8 @@ struct SieveArgs {
   uint32_t want_large;      // record large gaps
   uint32_t large_min_gap;   // 0: the reference's rule (gap >= 500 or merit >= 10); else every gap >= it
   uint32_t b_mode;          // medium primes: 0 = thread per prime, 1 = lane per (prime, residue)
+  const uint32_t* gbm;      // large-prime bitmap of the launch (nullptr: none); ANDed in at fill
+  uint32_t scatter_first;   // primes with index >= this were applied by the pre-pass
   uint32_t* tile_counter;
   TilePartial* partials;
   unsigned long long* acc;  // n_intervals * kAccStride
@@ -141,6 +153,8 @@ int launch_reduce(const SieveArgs& a, IntervalOut* out, void* stream);
 struct voss_interval_stats;
 namespace voss {
 int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_interval_stats* out, void* stream);
+int launch_scatter_large(const uint32_t* primes, const uint64_t* magic, uint32_t j0, uint32_t j1,
+                         const IntervalScatter* iv, uint32_t n_iv, uint32_t* gbm, int sm_count, void* stream);
 int sieve_kernel_attrs(int block, size_t smem, int* max_ctas_per_sm);
 void build_presieve_tables(uint32_t* out /* kPreWords */);
 int probe_smem_rmw(int sm_count, void* stream, float* ms, double* bytes);

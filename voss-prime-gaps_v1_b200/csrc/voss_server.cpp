@@ -275,6 +275,11 @@ Slot* make_slot(voss_server* S, int* rc) {
       (e = W.mr_in.ensure(8 * (C.max_batch_candidates + 1))) || (e = W.mr_out.ensure(C.max_batch_candidates + 1)) ||
       (e = W.mr_work.ensure(4 * (C.max_batch_candidates + 8))))
     return bad(e);
+  // the large-prime pre-pass bitmap: fixed size, never grown while serving
+  W.gbm_budget = C.max_batch_bitmap_bytes;
+  W.gbm_fixed = true;
+  if (W.gbm_budget && ((e = W.gbm.ensure(W.gbm_budget)) || (e = W.scat.ensure(sizeof(voss::IntervalScatter) * nreq))))
+    return bad(e);
   if (cudaMallocHost(&sl->h_istats, sizeof(voss_interval_stats) * nreq) != cudaSuccess ||
       cudaMallocHost(&sl->h_mr_in, 8 * (C.max_batch_candidates + 1)) != cudaSuccess ||
       cudaMallocHost(&sl->h_mr_out, C.max_batch_candidates + 1) != cudaSuccess ||
@@ -333,6 +338,7 @@ VOSS_API int voss_server_create(voss_ctx* ctx, const voss_server_config* cfg, vo
   if (!C.max_batch_requests) C.max_batch_requests = 1024;
   if (!C.max_batch_tiles) C.max_batch_tiles = 1u << 16;
   if (!C.max_batch_candidates) C.max_batch_candidates = 1ull << 22;
+  if (!C.max_batch_bitmap_bytes) C.max_batch_bitmap_bytes = 1ull << 30;
   if (C.slots > 64) return fail(VOSS_ERR_ARG, "at most 64 slots");
   if (C.max_batch_candidates > 0xFFFFFFF0ull) return fail(VOSS_ERR_ARG, "max_batch_candidates too large");
   for (uint32_t i = 0; i < C.slots; ++i) {

@@ -69,7 +69,8 @@ class Tuning(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [
         ("slots", c_uint32), ("max_batch_requests", c_uint32), ("max_batch_tiles", c_uint32),
-        ("fail_every_n_batches", c_uint32), ("max_batch_candidates", c_uint64), ("reserved", c_uint64 * 2),
+        ("fail_every_n_batches", c_uint32), ("max_batch_candidates", c_uint64), ("max_batch_bitmap_bytes", c_uint64),
+        ("reserved", c_uint64 * 1),
     ]
 
 

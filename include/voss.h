@@ -223,6 +223,37 @@ VOSS_API int voss_stats_merge(const voss_range_stats* parts, uint32_t n, voss_ra
                               voss_large_gap* large, uint64_t n_large, uint64_t large_cap,
                               uint64_t* large_written);
 
+/* ---- segment-level features: gap sequence, checkpoint / resume ------------------- */
+/* The sampled gap sequence of gap_sequence.csv (src/voss_v7_live.cu:234-253,526-547): for each
+ * segment s of [1, n] of length seg_num, per_seg = seq_size / NUM_SEG consecutive gaps starting
+ * at the middle prime (by count) of the segment's primes >= 7, at indices s*per_seg ...;
+ * gap[i] = p_next - p, p_lo[i] = p; unwritten entries are 0 (the reference leaves them
+ * uninitialised).  *written receives the number of gaps written. */
+VOSS_API int voss_gap_sequence(voss_ctx* ctx, uint64_t n, uint64_t seg_num, uint64_t seq_size,
+                               int32_t* gap, uint64_t* p_lo, uint64_t* written);
+/* gap_sequence.csv "index,gap,p" rows for gap[i] > 0 (src/voss_v7_live.cu:786-803). */
+VOSS_API int voss_write_gap_sequence(const int32_t* gap, const uint64_t* p_lo, uint64_t seq_size,
+                                     const char* dir);
+
+/* Statistics of one segment [lo, hi) into out/large: the unit of work of a checkpointed run. */
+typedef int (*voss_segment_fn)(void* user, uint64_t lo, uint64_t hi, voss_range_stats* out,
+                               voss_large_gap* large, uint64_t large_cap, uint64_t* large_written);
+/* [1, n] segment by segment (segments of seg_num integers, a multiple of 30), merging each into
+ * the running statistics; dir/checkpoint.bin is saved after the first, the last and every
+ * ckpt_every-th segment (src/voss_v7_live.cu:599-602) and holds every accumulator, so a resumed
+ * run equals an uninterrupted one; if dir/stop.txt exists at a save, it is removed and the call
+ * returns VOSS_ERR_STOPPED (:603-620).  A valid checkpoint for the same (n, seg_num, flags) is
+ * resumed from (*resumed_from = its next segment); the file is removed on success. */
+VOSS_API int voss_run_checkpointed(voss_ctx* ctx, uint64_t n, uint64_t seg_num, uint32_t flags,
+                                   uint32_t ckpt_every, const char* dir, voss_range_stats* out,
+                                   voss_large_gap* large, uint64_t large_cap, uint64_t* large_written,
+                                   uint64_t* resumed_from);
+/* The same driver over any segment function (the device sieve in voss_run_checkpointed). */
+VOSS_API int voss_run_checkpointed_fn(voss_segment_fn fn, void* user, uint64_t n, uint64_t seg_num,
+                                      uint32_t flags, uint32_t ckpt_every, const char* dir,
+                                      voss_range_stats* out, voss_large_gap* large, uint64_t large_cap,
+                                      uint64_t* large_written, uint64_t* resumed_from);
+
 /* ---- serving: continuous batching ------------------------------------------------ */
 /* A request server over one context.  Client threads submit interval-sieve + gap-statistics
  * requests and Miller-Rabin batches; a scheduler thread launches the pending requests, in

@@ -16,7 +16,8 @@ import oracle_lib as O
 pytestmark = pytest.mark.gpu
 
 SEG = 30_000_000_000
-EXACT = ["gap_histogram.csv", "hl_trend.csv", "modq_counts.csv", "modq_gap_hist.csv", "chebyshev.csv"]
+EXACT = ["gap_histogram.csv", "hl_trend.csv", "modq_counts.csv", "modq_gap_hist.csv", "chebyshev.csv",
+         "gap_sequence.csv"]
 
 
 @pytest.mark.parametrize("n", [10**9, 10**10, 10**11])
@@ -30,6 +31,8 @@ def test_artifacts_equal_reference_program(gpu_ctx, n):
         assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
         res = gpu_ctx.sieve_range(1, n + 1, compat=True, seg_num=SEG, large_cap=50_000_000)
         voss.write_artifacts(res, our_dir)
+        gap, p = gpu_ctx.gap_sequence(n, SEG, 5_000_000)
+        voss.write_gap_sequence(gap, p, our_dir)
         m = re.search(r"Total primes:\s*(\d+)", r.stdout)
         assert m and int(m.group(1)) == res.prime_count
         for name in EXACT:

@@ -7,7 +7,7 @@ behind a C ABI, include/voss.h); this package is its ctypes face.
 from ._native import (FLAG_REF_COMPAT, IHIST, MAX_GAP, MODQ_MAX_GAP, Q_LIST, VossError, lib_path,  # noqa: F401
                       load)
 from .api import (INTERVAL_DTYPE, LARGE_DTYPE, Context, RangeResult, device_count, merge_stats,  # noqa: F401
-                  range_result, to_struct, version, write_artifacts)
+                  range_result, run_checkpointed_fn, to_struct, version, write_artifacts, write_gap_sequence)
 
 __all__ = [
     "Context", "RangeResult", "VossError", "merge_stats", "write_artifacts", "device_count", "version",

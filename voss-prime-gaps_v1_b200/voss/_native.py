@@ -82,6 +82,10 @@ class ServerStats(ctypes.Structure):
     ]
 
 
+SEGMENT_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_uint64, c_uint64, POINTER(RangeStats), POINTER(LargeGap),
+                              c_uint64, POINTER(c_uint64))
+
+
 # name -> (restype, argtypes); every entry point declared in include/voss.h
 SIGNATURES = {
     "voss_version": (c_char_p, []),
@@ -108,6 +112,14 @@ SIGNATURES = {
     "voss_write_artifacts": (c_int, [POINTER(RangeStats), POINTER(LargeGap), c_uint64, c_char_p]),
     "voss_stats_merge": (c_int, [POINTER(RangeStats), c_uint32, POINTER(RangeStats), POINTER(LargeGap),
                                  c_uint64, c_uint64, POINTER(c_uint64)]),
+    "voss_gap_sequence": (c_int, [c_void_p, c_uint64, c_uint64, c_uint64, POINTER(c_int32), POINTER(c_uint64),
+                                  POINTER(c_uint64)]),
+    "voss_write_gap_sequence": (c_int, [POINTER(c_int32), POINTER(c_uint64), c_uint64, c_char_p]),
+    "voss_run_checkpointed": (c_int, [c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, c_char_p, POINTER(RangeStats),
+                                      POINTER(LargeGap), c_uint64, POINTER(c_uint64), POINTER(c_uint64)]),
+    "voss_run_checkpointed_fn": (c_int, [SEGMENT_FN, c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, c_char_p,
+                                         POINTER(RangeStats), POINTER(LargeGap), c_uint64, POINTER(c_uint64),
+                                         POINTER(c_uint64)]),
     "voss_server_create": (c_int, [c_void_p, POINTER(ServerConfig), POINTER(c_void_p)]),
     "voss_server_destroy": (None, [c_void_p]),
     "voss_server_submit_interval": (c_int, [c_void_p, c_uint64, c_uint64, POINTER(c_uint64)]),

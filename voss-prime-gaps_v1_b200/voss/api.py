@@ -182,6 +182,28 @@ class Context:
                                               out.ctypes.data_as(ctypes.POINTER(N.IntervalStats))))
         return out
 
+    def gap_sequence(self, n: int, seg_num: int = 30_000_000_000, seq_size: int = 5_000_000):
+        """voss_gap_sequence: the reference's sampled gap sequence of [1, n] (gap, lower prime)."""
+        gap = np.zeros(seq_size, dtype=np.int32)
+        p = np.zeros(seq_size, dtype=np.uint64)
+        w = c_uint64()
+        N.check(self.lib.voss_gap_sequence(self._h, n, seg_num, seq_size,
+                                           gap.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _u64p(p), byref(w)))
+        return gap, p
+
+    def run_checkpointed(self, n: int, seg_num: int = 30_000_000_000, compat: bool = True, ckpt_every: int = 5,
+                         directory: str = ".", large_cap: int = 1 << 22):
+        """voss_run_checkpointed: [1, n] segment by segment with checkpoint.bin / stop.txt in
+        `directory`.  Returns (RangeResult, resumed_from); raises VossError(-7) when stopped."""
+        st = N.RangeStats()
+        large = np.zeros(large_cap, dtype=LARGE_DTYPE)
+        w, res = c_uint64(), c_uint64()
+        N.check(self.lib.voss_run_checkpointed(self._h, n, seg_num, N.FLAG_REF_COMPAT if compat else 0, ckpt_every,
+                                               directory.encode(), byref(st),
+                                               large.ctypes.data_as(ctypes.POINTER(N.LargeGap)), large_cap,
+                                               byref(w), byref(res)))
+        return range_result(st, large[: w.value].copy()), res.value
+
     # -- Miller-Rabin / proofs --------------------------------------------------------------
     def mr_verify(self, n) -> np.ndarray:
         n = np.ascontiguousarray(n, dtype=np.uint64)
@@ -245,6 +267,44 @@ def merge_stats(parts: list[RangeResult], large_cap: int | None = None) -> Range
     N.check(lib.voss_stats_merge(arr, len(parts), byref(out), large.ctypes.data_as(ctypes.POINTER(N.LargeGap)),
                                  min(large_in.size, cap), cap, byref(w)))
     return range_result(out, large[: w.value].copy())
+
+
+def write_gap_sequence(gap, p, out_dir: str) -> None:
+    """voss_write_gap_sequence: gap_sequence.csv rows for the written entries."""
+    gap = np.ascontiguousarray(gap, dtype=np.int32)
+    p = np.ascontiguousarray(p, dtype=np.uint64)
+    N.check(N.load().voss_write_gap_sequence(gap.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _u64p(p), gap.size,
+                                             out_dir.encode()))
+
+
+def run_checkpointed_fn(segment, n: int, seg_num: int, compat: bool, ckpt_every: int, directory: str,
+                        large_cap: int = 1 << 22):
+    """voss_run_checkpointed_fn over a Python segment function segment(lo, hi) -> RangeResult
+    (any source of statistics: the device, or a CPU oracle in tests)."""
+    lib = N.load()
+
+    def cb(user, lo, hi, out, large, cap, written):
+        try:
+            r = segment(lo, hi)
+            st = r.raw if r.raw is not None else to_struct(r)
+            ctypes.memmove(out, ctypes.byref(st), ctypes.sizeof(N.RangeStats))
+            k = min(cap, r.large.size)
+            if k:
+                ctypes.memmove(large, np.ascontiguousarray(r.large[:k]).ctypes.data, k * LARGE_DTYPE.itemsize)
+            written[0] = k
+            return 0
+        except Exception:
+            return -9
+
+    fn = N.SEGMENT_FN(cb)
+    st = N.RangeStats()
+    large = np.zeros(large_cap, dtype=LARGE_DTYPE)
+    w, res = c_uint64(), c_uint64()
+    N.check(lib.voss_run_checkpointed_fn(fn, None, n, seg_num, N.FLAG_REF_COMPAT if compat else 0, ckpt_every,
+                                         directory.encode(), byref(st),
+                                         large.ctypes.data_as(ctypes.POINTER(N.LargeGap)), large_cap, byref(w),
+                                         byref(res)))
+    return range_result(st, large[: w.value].copy()), res.value
 
 
 NOALLOC_MAX_COUNT = 1 << 22

@@ -110,4 +110,4 @@ def report_lines(res, total_s: float, phases: list[tuple[str, float]], written: 
 
 
 WRITTEN = ["OK gap_histogram.csv", "OK hl_trend.csv (hybrid)", "OK modq_counts.csv", "OK modq_gap_hist.csv",
-           "OK chebyshev.csv"]
+           "OK chebyshev.csv", "OK gap_sequence.csv"]

@@ -4,10 +4,12 @@
 The reference rewrites N/SEG_NUM/MAX_POS into src/voss_v7_live.cu, compiles it with nvcc, runs
 the binary in RESULTS and parses its stdout (src/voss_master.py:88-179).  This driver keeps the
 same module constants (run_voss.py:111-123 rewrites `N_VALUE = ...` and `SEG_NUM = ...` in this
-file the same way), the same OEIS check and the same artifacts, but computes everything with one
-call into libvoss.so (voss_sieve_range in reference-compat mode) and writes the CSVs with
-voss_write_artifacts.  It prints the reference program's report block, so the `Total primes:`
-line that the reference parses is there too.
+file the same way), the same OEIS check and the same artifacts, but computes everything in
+libvoss.so: the range segment by segment with checkpoint.bin / stop.txt in RESULTS
+(voss_run_checkpointed, reference-compat statistics), the sampled gap sequence
+(voss_gap_sequence), and the CSVs (voss_write_artifacts, voss_write_gap_sequence).  It prints
+the reference program's report block, so the `Total primes:` line that the reference parses is
+there too.
 
 Placement: copy it over src/voss_master.py of the reference tree (ROOT is the parent of the
 directory holding this file, as in the reference) and make the `voss` package importable
@@ -33,6 +35,7 @@ N_VALUE = 1000000000000    # 10^12
 SEG_NUM = 30000000000      # 3x10^10 (the reference's segment length; used for its artifact rules)
 
 MAX_LARGE_GAPS = 50_000_000  # src/voss_v7_live.cu:34
+GAP_SEQ_SIZE = 5_000_000     # src/voss_v7_live.cu:35
 
 
 def _import_voss():
@@ -79,16 +82,31 @@ def run(n: int = None, seg_num: int = None, results: str = None, device: int = 0
     results = RESULTS if results is None else results
     os.makedirs(results, exist_ok=True)
     t0 = time.perf_counter()
+    num_seg = (n + seg_num - 1) // seg_num
     with voss.Context(n + 1, device=device) as ctx:
+        # segment by segment with checkpoint.bin / stop.txt in the results directory, as the
+        # reference program keeps them in its working directory (src/voss_v7_live.cu:407-421,599-621)
         cap = 1 << 22
-        res = ctx.sieve_range(1, n + 1, compat=True, seg_num=seg_num, large_cap=cap)
+        try:
+            res, resumed = ctx.run_checkpointed(n, seg_num, compat=True, ckpt_every=5, directory=results, large_cap=cap)
+        except voss.VossError as e:
+            if e.code == -7:  # stop file: checkpoint saved, clean exit (:603-620)
+                print(f"\n>>> STOP-FILE detected — exiting cleanly <<<")
+                return {"prime_count": None, "total_s": time.perf_counter() - t0, "result": None, "stopped": True}
+            raise
+        if resumed:
+            print(f">>> RESUMING FROM SEGMENT {resumed} / {num_seg} <<<")
+        else:
+            print(">>> STARTING FRESH <<<")
         if res.large_total > cap:
             cap = min(int(res.large_total), MAX_LARGE_GAPS)
             res = ctx.sieve_range(1, n + 1, compat=True, seg_num=seg_num, large_cap=cap)
-        sieve_ms, total_ms = ctx.last_kernel_ms()
+        t_sieve = time.perf_counter() - t0
+        gap, p = ctx.gap_sequence(n, seg_num, GAP_SEQ_SIZE)
     total_s = time.perf_counter() - t0
     voss.write_artifacts(res, results)
-    phases = [("Sieve", sieve_ms / 1e3), ("Stitch", (total_ms - sieve_ms) / 1e3)]
+    voss.write_gap_sequence(gap, p, results)
+    phases = [("Sieve", t_sieve), ("GapSeq", total_s - t_sieve)]
     for line in report_lines(res, total_s, phases, WRITTEN):
         print(line)
     print("\nDone.")

@@ -30,6 +30,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import re
 import statistics
@@ -137,13 +138,38 @@ def measured_peaks() -> dict:
 
 def profile_traffic_per_unit() -> tuple[float | None, str | None]:
     """DRAM bytes per sieved integer of sieve_tiles_kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "sieve_tiles_kernel_1e11.md")
+    rel = os.path.join("profiles", "sieve_tiles_kernel_1e11.md")
     try:
-        txt = open(p).read()
+        txt = open(os.path.join(ROOT, rel)).read()
     except OSError:
         return None, None
     m = re.search(r"dram_bytes_per_integer:\s*([0-9.eE+-]+)", txt)
-    return (float(m.group(1)), p) if m else (None, None)
+    return (float(m.group(1)), rel + " (10^11 capture, scaled by integers)") if m else (None, None)
+
+
+_COPRIME30 = [sum(1 for r in range(1, x + 1) if r % 2 and r % 3 and r % 5) for x in range(30)]
+
+
+def sieve_work(n: int) -> int:
+    """H(n): bit-clears of the wheel-30 sieve of [1, n] — for every prime 7 <= p <= isqrt(n),
+    the multiples of p in [p^2, n] that are coprime to 30 (the reference's per-prime start
+    rule, voss_v7_live.cu:449-478).  Numpy, so the roofline needs nothing from the oracle."""
+    import numpy as np
+    s = math.isqrt(n)
+    if s < 7:
+        return 0
+    flags = np.ones(s + 1, dtype=bool)
+    flags[:2] = False
+    for q in range(2, math.isqrt(s) + 1):
+        if flags[q]:
+            flags[q * q::q] = False
+    p = np.nonzero(flags)[0].astype(np.int64)
+    p = p[p >= 7]
+    table = np.asarray(_COPRIME30, dtype=np.int64)
+
+    def upto(x):
+        return 8 * (x // 30) + table[x % 30]
+    return int((upto(n // p) - upto(p - 1)).sum())
 
 
 # ---------------------------------------------------------------------------------------
@@ -520,8 +546,7 @@ def main():
     value = total_range / (step_ms * 1e-3)
     # algorithmic bytes of the dominant kernel: 8 B per bit-clear (32-bit RMW) + one read of
     # the bitmap (N/30 B) by the extraction, for this rank's range
-    import oracle_lib as O
-    h = O.sieve_work(hi - 1) - (O.sieve_work(lo - 1) if lo > 1 else 0)
+    h = sieve_work(hi - 1) - (sieve_work(lo - 1) if lo > 1 else 0)
     alg_bytes = 8.0 * h + (hi - lo) / 30.0
     smem_peak = ctx.probe_smem_rmw()
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9

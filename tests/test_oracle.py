@@ -9,6 +9,8 @@ import pytest
 
 import oracle_lib as O
 
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")))
 SEG = 30_000_000_000
 
@@ -76,6 +78,17 @@ def test_hist_1000_and_chebyshev_1e9():
 def test_sieve_work_matches_baseline_table():
     assert O.sieve_work(10**9) == 404309576
     assert O.sieve_work(10**12) == 484385202990
+
+
+def test_bench_sieve_work_equals_oracle():
+    """bench.py's roofline counts H(n) with its own numpy statement; it must equal the
+    oracle's count, including the difference form used for a rank's sub-range."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    for n in (1, 48, 49, 50, 10**6 + 7, 10**9, 2 * 10**12, 10**12):
+        assert bench.sieve_work(n) == O.sieve_work(n), n
 
 
 @pytest.mark.parametrize("lo,hi,compat,seg", [

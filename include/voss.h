@@ -119,7 +119,9 @@ typedef struct voss_tuning {
   uint32_t coop_div;        /* primes p < tile_bytes/coop_div are cleared warp-cooperatively */
   uint32_t mult_factor;     /* primes p >= mult_factor*tile_bytes use the multiples walk */
   uint32_t medium_mode;     /* other primes: 0 = a thread per prime, 1 = a lane per (prime, residue) */
-  uint32_t reserved[2];
+  uint32_t walk_sixteenths; /* mode 0: primes p >= walk_sixteenths*tile_bytes/16 walk their coprime
+                               multiples instead of 8 residue progressions (>= 16*mult_factor: never) */
+  uint32_t reserved[1];
 } voss_tuning;
 
 typedef struct voss_ctx voss_ctx;

@@ -37,6 +37,13 @@ namespace voss {
 __constant__ uint8_t c_wheel_step[64];
 // residue r (mod 30) -> wheel bit index, or -1 when gcd(r, 30) > 1.
 __constant__ int8_t c_res_bit[32];
+// Wheel walk of a prime p = 30a + W30[bi] over its multiples p*m with gcd(m, 30) = 1.
+// [bi*30 + t]: t = (offset of the first multiple of p at or above a tile's start) mod 30 gives
+// m mod 30 = t * p^-1 (mod 30); stored: (steps to the next m coprime to 30) | (its wheel index << 3).
+__constant__ uint8_t c_walk_start[240];
+// [bi*8 + j]: from m = 30c + W30[j] to the next coprime m, the byte index of p*m grows by
+// a*gap_j + corr (gap_j = W30[j+1] - W30[j], W30[8] = 31); stored: bit of p*m | corr << 3 | gap_j/2 << 6.
+__constant__ uint8_t c_walk_step[64];
 
 static int ensure_tables();
 
@@ -106,6 +113,74 @@ __device__ __forceinline__ void clear_bit_word(uint32_t* bm, uint32_t word, uint
   atomicAnd(bm + word, mask);
 }
 
+// Clears bit `bit` of every byte start, start + 32p, start + 64p, ... below Lt (one lane of a
+// warp-cooperative small prime).  The stride is a multiple of 4 bytes, so the byte lane inside the
+// word, and with it the mask, never changes; four clears per loop trip.
+__device__ __forceinline__ void clear_lane_progression(uint32_t* bm, uint32_t start, uint32_t p,
+                                                       uint32_t bit, uint32_t Lt, uint32_t nw,
+                                                       uint32_t* err) {
+  const uint32_t mask = ~(1u << (((start & 3u) << 3) | bit));
+  const uint32_t ws = 8u * p;                           // 32p bytes
+  const uint32_t wlim = (Lt + 3u - (start & 3u)) >> 2;  // start + 4k < Lt  <=>  (start >> 2) + k < wlim
+  uint32_t w = start >> 2;
+  if (wlim > 3u * ws) {
+    const uint32_t wlim4 = wlim - 3u * ws;
+    for (; w < wlim4; w += 4u * ws) {
+      clear_bit_word(bm, w, mask, nw, err);
+      clear_bit_word(bm, w + ws, mask, nw, err);
+      clear_bit_word(bm, w + 2u * ws, mask, nw, err);
+      clear_bit_word(bm, w + 3u * ws, mask, nw, err);
+    }
+  }
+  for (; w < wlim; w += ws) clear_bit_word(bm, w, mask, nw, err);
+}
+
+// Clears bit `bit` of bytes byte, byte + p, byte + 2p, ... below Lt (p odd).  Four consecutive
+// hits fall in the four distinct byte lanes of their words, and advancing all four by 4p bytes
+// moves each by exactly p words, so the unrolled loop keeps four fixed masks and word offsets.
+__device__ __forceinline__ void clear_progression(uint32_t* bm, uint32_t byte, uint32_t p, uint32_t bit,
+                                                  uint32_t Lt, uint32_t nw, uint32_t* err) {
+  if (byte + 3u * p < Lt) {
+    const uint32_t b1 = byte + p, b2 = b1 + p, b3 = b2 + p;
+    const uint32_t m0 = ~(1u << (((byte & 3u) << 3) | bit)), m1 = ~(1u << (((b1 & 3u) << 3) | bit));
+    const uint32_t m2 = ~(1u << (((b2 & 3u) << 3) | bit)), m3 = ~(1u << (((b3 & 3u) << 3) | bit));
+    uint32_t w0 = byte >> 2;
+    const uint32_t d1 = (b1 >> 2) - w0, d2 = (b2 >> 2) - w0, d3 = (b3 >> 2) - w0;
+    // b3 + 4pk < Lt  <=>  w0 + k < lim  (w0 + d3 = b3 >> 2)
+    const uint32_t lim = ((Lt + 3u - (b3 & 3u)) >> 2) - d3;
+    uint32_t k = 0;
+    for (; w0 < lim; w0 += p, ++k) {
+      clear_bit_word(bm, w0, m0, nw, err);
+      clear_bit_word(bm, w0 + d1, m1, nw, err);
+      clear_bit_word(bm, w0 + d2, m2, nw, err);
+      clear_bit_word(bm, w0 + d3, m3, nw, err);
+    }
+    byte += 4u * p * k;
+  }
+  for (; byte < Lt; byte += p) clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
+}
+
+// Clears every multiple p*m (gcd(m, 30) = 1) of prime p = 30a + W30[bi] in the tile whose first
+// integer is vbase (a multiple of 30) and whose length is Lt bytes, visiting only those multiples
+// (about 8*Lt/p of them) instead of eight residue progressions.  rv = vbase mod p.
+__device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t p, uint32_t a, uint32_t bi, uint32_t rv,
+                                                 const uint8_t* s_wstart, const uint8_t* s_wstep,
+                                                 uint32_t Lt, uint32_t nw, uint32_t* err) {
+  uint32_t off = rv ? p - rv : 0u;         // first multiple of p at or above vbase, as an offset
+  const uint32_t t = off - 30u * (off / 30u);
+  const uint32_t st = s_wstart[bi * 30u + t];
+  off += (st & 7u) * p;                     // first multiple with m coprime to 30
+  uint32_t j = st >> 3;
+  uint32_t byte = off / 30u;
+  const uint8_t* row = s_wstep + bi * 8u;
+  while (byte < Lt) {
+    const uint32_t e = row[j];
+    clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | (e & 7u))), nw, err);
+    byte += a * ((e >> 5) & 6u) + ((e >> 3) & 7u);
+    j = (j + 1u) & 7u;
+  }
+}
+
 __device__ __forceinline__ void sm_add(uint32_t* cnt, uint32_t idx, uint32_t* err) {
   VOSS_SM_GUARD(idx, (uint32_t)kSmCounters)
   atomicAdd(cnt + idx, 1u);
@@ -148,7 +223,7 @@ __device__ unsigned long long g_phase_cycles[16];
 
 struct TileHdr {
   unsigned long long ktile, vbase, vlo, vhi, seg_k;
-  uint32_t nw, lt, np, ia, ib, vb, gthr, k28, k143;
+  uint32_t nw, lt, np, ia, ib, iw, vb, gthr, k28, k143;
   uint32_t pre_base[kPreGroups];
   uint32_t interval, tile, next_tile, cur_iv, since_flush, flush;
   uint32_t r0, r1;       // base primes lying in the tile (restore)
@@ -262,8 +337,17 @@ __device__ __forceinline__ void block_reduce_tile(uint32_t cnt, unsigned long lo
   }
 }
 
+// Accumulator word of shared counter i.  The class counters fold: shared class c of the
+// (k mod 28) block is class c mod 28, of the (k mod 143) block class c mod 143.
 __device__ __forceinline__ uint32_t acc_index(uint32_t i) {
-  return i < (uint32_t)kSmModq ? (uint32_t)kAccHist + i : (uint32_t)kAccModq + (i - (uint32_t)kSmModq);
+  if (i < (uint32_t)kSmModq) return (uint32_t)kAccHist + i;
+  if (i < (uint32_t)kSmCls28) return (uint32_t)kAccModq + (i - (uint32_t)kSmModq);
+  if (i < (uint32_t)kSmCls143) {
+    const uint32_t c = (i - (uint32_t)kSmCls28) >> 3;
+    return (uint32_t)kAccCls28 + 8u * (c >= 28u ? c - 28u : c) + (i & 7u);
+  }
+  const uint32_t c = (i - (uint32_t)kSmCls143) >> 3;
+  return (uint32_t)kAccCls143 + 8u * (c >= 143u ? c - 143u : c) + (i & 7u);
 }
 
 constexpr uint32_t kFlushEvery = 2048;  // tiles between counter flushes (u32 headroom)
@@ -281,12 +365,18 @@ sieve_tiles_kernel(SieveArgs a) {
   // would serialize in the constant cache.
   __shared__ uint8_t s_step[64];
   __shared__ int8_t s_rb[32];
+  __shared__ uint32_t s_pos[32];  // bit b of a word -> integer offset 30 * (b / 8) + W30[b % 8]
+  __shared__ uint8_t s_wstart[240];
+  __shared__ uint8_t s_wstep[64];
   uint32_t* err = a.error;
 
   const int tid = threadIdx.x, lane = tid & 31;
   for (uint32_t i = tid; i < kPreWords; i += BLOCK) pre[i] = a.pretab[i];
   if (tid < 64) s_step[tid] = c_wheel_step[tid];
   if (tid < 32) s_rb[tid] = c_res_bit[tid];
+  if (tid < 32) s_pos[tid] = 30u * ((uint32_t)tid >> 3) + w30((uint32_t)tid & 7u);
+  if (tid < 240) s_wstart[tid] = c_walk_start[tid];
+  if (tid < 64) s_wstep[tid] = c_walk_step[tid];
   if (!EMIT)
     for (uint32_t i = tid; i < (uint32_t)kSmCounters; i += BLOCK) cnt[i] = 0;
   if (tid == 0) {
@@ -359,6 +449,8 @@ sieve_tiles_kernel(SieveArgs a) {
       uint32_t ib = count_lt(a.primes, np, (uint64_t)H.lt * a.mult_factor);
       H.ia = ia;
       H.ib = ib < ia ? ia : ib;
+      const uint32_t iw = count_lt(a.primes, np, ((uint64_t)H.lt * a.walk_sixteenths) >> 4);
+      H.iw = iw < H.ia ? H.ia : (iw > H.ib ? H.ib : iw);
       H.r0 = count_lt(a.primes, a.n_primes, H.vbase);
       H.r1 = count_lt(a.primes, a.n_primes, H.vbase + 30ull * H.lt);
       uint32_t vb = kNone;
@@ -417,7 +509,7 @@ sieve_tiles_kernel(SieveArgs a) {
     // ---- 2. sieve ----------------------------------------------------------------------
     {
       const uint64_t ktile = H.ktile;
-      const uint32_t ia = H.ia, ib = H.ib, np = H.np;
+      const uint32_t ia = H.ia, ib = H.ib, iw = H.iw, np = H.np;
       // small primes: a warp per prime
       for (;;) {
         uint32_t i = 0;
@@ -427,15 +519,12 @@ sieve_tiles_kernel(SieveArgs a) {
         const uint32_t p = a.primes[i];
         const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
         const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
-        const uint32_t stride = 32u * p;
 #pragma unroll 1
         for (uint32_t o = 0; o < 8; ++o) {
           const uint32_t e = s_step[bi * 8u + o];
           const uint32_t delta = pa * w30(o) + (e & 31u);
-          uint32_t s = delta >= r ? delta - r : delta + p - r;
-          uint32_t byte = s + (uint32_t)lane * p;
-          const uint32_t mask = ~(1u << (((byte & 3u) << 3) | (e >> 5)));
-          for (; byte < Lt; byte += stride) clear_bit_word(bm, byte >> 2, mask, nw, err);
+          const uint32_t s = delta >= r ? delta - r : delta + p - r;
+          clear_lane_progression(bm, s + (uint32_t)lane * p, p, e >> 5, Lt, nw, err);
         }
       }
       VOSS_PHASE(3)
@@ -448,7 +537,12 @@ sieve_tiles_kernel(SieveArgs a) {
           base = __shfl_sync(0xFFFFFFFFu, base, 0);
           if (base >= ib - ia) break;
           const uint32_t i = ia + base + (uint32_t)lane;
-          if (i < ib) {
+          if (i >= iw && i < ib) {
+            // few hits per tile: walk the prime's coprime multiples
+            const uint32_t p = a.primes[i];
+            const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
+            clear_wheel_walk(bm, p, pa, bi, mod_barrett(H.vbase, p, a.magic[i]), s_wstart, s_wstep, Lt, nw, err);
+          } else if (i < ib) {
             const uint32_t p = a.primes[i];
             const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
             const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
@@ -456,10 +550,7 @@ sieve_tiles_kernel(SieveArgs a) {
             for (uint32_t o = 0; o < 8; ++o) {
               const uint32_t e = s_step[bi * 8u + o];
               const uint32_t delta = pa * w30(o) + (e & 31u);
-              uint32_t byte = delta >= r ? delta - r : delta + p - r;
-              const uint32_t bit = e >> 5;
-              for (; byte < Lt; byte += p)
-                clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
+              clear_progression(bm, delta >= r ? delta - r : delta + p - r, p, e >> 5, Lt, nw, err);
             }
           }
         }
@@ -477,10 +568,7 @@ sieve_tiles_kernel(SieveArgs a) {
             const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
             const uint32_t e = s_step[bi * 8u + o];
             const uint32_t delta = pa * wo + (e & 31u);
-            uint32_t byte = delta >= r ? delta - r : delta + p - r;
-            const uint32_t bit = e >> 5;
-            for (; byte < Lt; byte += p)
-              clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
+            clear_progression(bm, delta >= r ? delta - r : delta + p - r, p, e >> 5, Lt, nw, err);
           }
         }
       }
@@ -570,57 +658,54 @@ sieve_tiles_kernel(SieveArgs a) {
       int32_t prev = block_excl_max<BLOCK>(my_last, S, &tile_last);
       VOSS_PHASE(7)
 
-      // pass 2: walk the chunk in order
+      // pass 2: walk the chunk in order.  The class counters of a word's 4 bytes are indexed
+      // without wrapping (k mod 28 + j up to 30, k mod 143 + j up to 145: 31 and 146 classes);
+      // the flush folds the tail classes back.  That makes both class indices one add per prime.
       const uint32_t vb = H.vb;
       const uint32_t gthr = H.gthr;
-      uint32_t k28 = (H.k28 + 4u * c0) % 28u;
-      uint32_t k143 = (H.k143 + 4u * c0) % 143u;
+      uint32_t c28 = (uint32_t)kSmCls28 + 8u * ((H.k28 + 4u * c0) % 28u);
+      uint32_t c143 = (uint32_t)kSmCls143 + 8u * ((H.k143 + 4u * c0) % 143u);
       uint32_t my_cnt = 0, mg = 0, mlo = 0;
-      uint32_t o_prev = 0;
+      uint32_t mq_prev = 0;  // modq row of the previous prime
       if (prev >= 0) {
         const uint32_t kp = (uint32_t)prev / 30u;
-        o_prev = (uint32_t)s_rb[(uint32_t)prev - 30u * kp];
+        mq_prev = (uint32_t)kSmModq + kModqBins * (uint32_t)s_rb[(uint32_t)prev - 30u * kp];
       }
       uint32_t w = c0;
       uint32_t x = w < cend ? bm[w] : 0u;
+      uint32_t wpos = 120u * w;
       for (;;) {
         while (x == 0u) {
           if (++w >= cend) break;
           x = bm[w];
-          k28 += 4u;
-          if (k28 >= 28u) k28 -= 28u;
-          k143 += 4u;
-          if (k143 >= 143u) k143 -= 143u;
+          wpos += 120u;
+          c28 += 32u;
+          if (c28 >= (uint32_t)kSmCls28 + 224u) c28 -= 224u;
+          c143 += 32u;
+          if (c143 >= (uint32_t)kSmCls143 + 1144u) c143 -= 1144u;
         }
         if (w >= cend) break;
         const uint32_t b = (uint32_t)__ffs(x) - 1u;
         x &= x - 1u;
-        const uint32_t j = b >> 3, o = b & 7u;
-        const uint32_t pos = 120u * w + 30u * j + w30(o);
+        const uint32_t pos = wpos + s_pos[b];
         ++my_cnt;
-        uint32_t c = k28 + j;
-        if (c >= 28u) c -= 28u;
-        sm_add(cnt, kSmCls28 + c * 8u + o, err);
-        c = k143 + j;
-        if (c >= 143u) c -= 143u;
-        sm_add(cnt, kSmCls143 + c * 8u + o, err);
+        sm_add(cnt, c28 + b, err);
+        sm_add(cnt, c143 + b, err);
+        const uint32_t mq = (uint32_t)kSmModq + kModqBins * (b & 7u);
         if (prev >= 0) {
           const uint32_t g = pos - (uint32_t)prev;
           const bool crossing = ((uint32_t)prev < vb) && (pos >= vb);
-          if (g < 100u && !crossing) {
-            sm_add(cnt, kSmModq + o_prev * kModqBins + (g >> 1), err);
-          } else if (g < 2u * kHistBins) {
-            sm_add(cnt, kSmHist + (g >> 1), err);
+          const bool small = g < 100u && !crossing;
+          if (small || g < 2u * kHistBins) {
+            sm_add(cnt, (small ? mq_prev : (uint32_t)kSmHist) + (g >> 1), err);
           } else {
             atomicAdd(a.acc + (size_t)H.cur_iv * kAccStride + kAccHistOver, 1ull);
             const uint32_t slot = atomicAdd(a.over_count, 1u);
             if (slot < a.over_cap) a.over[slot] = OverflowGap{H.cur_iv, g};
             else atomicOr(err, kErrOverflowList);
           }
-          if (g > mg) {
-            mg = g;
-            mlo = (uint32_t)prev;
-          }
+          mlo = g > mg ? (uint32_t)prev : mlo;
+          mg = g > mg ? g : mg;
           const bool cand = a.large_min_gap ? (g >= a.large_min_gap) : (g > 100u && (g >= 500u || g >= gthr));
           if (a.want_large && cand && !crossing) {
             const uint64_t v0 = H.vbase + (uint32_t)prev;
@@ -637,7 +722,7 @@ sieve_tiles_kernel(SieveArgs a) {
           H.first = pos;  // exactly one thread meets a prime with no predecessor in the tile
         }
         prev = (int32_t)pos;
-        o_prev = o;
+        mq_prev = mq;
       }
       const unsigned long long key =
           mg ? (((unsigned long long)mg << 32) | (unsigned long long)(0xFFFFFFFFu - mlo)) : 0ull;
@@ -907,6 +992,26 @@ static int ensure_tables() {
       const int bw = kW30h[bi] * kW30h[o];
       step[bi * 8 + o] = (uint8_t)((bw / 30) | (rb[bw % 30] << 5));
     }
+  uint8_t wstart[240], wstep[64];
+  for (int bi = 0; bi < 8; ++bi) {
+    int pinv = 1;
+    while ((kW30h[bi] * pinv) % 30 != 1) ++pinv;
+    for (int t = 0; t < 30; ++t) {
+      const int u = (t * pinv) % 30;
+      int adv = 0;
+      while (rb[(u + adv) % 30] < 0) ++adv;
+      wstart[bi * 30 + t] = (uint8_t)(adv | (rb[(u + adv) % 30] << 3));
+    }
+    for (int j = 0; j < 8; ++j) {
+      const int w = kW30h[bi];
+      const int d0 = (w * kW30h[j]) / 30;
+      const int gap = (j < 7 ? kW30h[j + 1] : 31) - kW30h[j];
+      const int corr = j < 7 ? (w * kW30h[j + 1]) / 30 - d0 : w + 0 - d0;  // j = 7: next m is 30(c+1) + 1
+      wstep[bi * 8 + j] = (uint8_t)(rb[(w * kW30h[j]) % 30] | (corr << 3) | ((gap / 2) << 6));
+    }
+  }
+  if (cudaMemcpyToSymbol(c_walk_start, wstart, sizeof(wstart)) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(c_walk_step, wstep, sizeof(wstep)) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_wheel_step, step, sizeof(step)) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_res_bit, rb, sizeof(rb)) != cudaSuccess) return -1;
   g_tables_ready.fetch_or(bit);

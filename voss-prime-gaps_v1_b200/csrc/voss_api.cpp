@@ -111,11 +111,15 @@ int apply_tuning(voss_ctx* c, const voss_tuning& t0) {
   voss_tuning t = t0;
   if (!t.block_threads) t.block_threads = 1024;
   if (!t.chunk_words) t.chunk_words = t.block_threads == 1024 ? 49 : 45;
-  if (!t.coop_div) t.coop_div = 48;
+  if (!t.coop_div) t.coop_div = 128;
   if (!t.mult_factor) t.mult_factor = 8;
+  if (!t.walk_sixteenths) t.walk_sixteenths = 4;
   if (t.block_threads != 512 && t.block_threads != 1024)
     return fail(VOSS_ERR_ARG, "block_threads must be 512 or 1024");
   if (t.medium_mode > 1) return fail(VOSS_ERR_ARG, "medium_mode must be 0 or 1");
+  // medium primes (p < mult_factor * tile bytes <= 64 * 1,044,480) keep 7p below 2^32 in the
+  // 32-bit offset arithmetic of their clearing loops
+  if (t.mult_factor > 64) return fail(VOSS_ERR_ARG, "mult_factor must be <= 64");
   if ((t.chunk_words & 1u) == 0 || t.chunk_words > 255)
     return fail(VOSS_ERR_ARG, "chunk_words must be odd and <= 255");
   const uint32_t tw = t.block_threads * t.chunk_words;
@@ -197,6 +201,7 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
   a.chunk_words = c->tune.chunk_words;
   a.coop_div = c->tune.coop_div;
   a.mult_factor = c->tune.mult_factor;
+  a.walk_sixteenths = c->tune.walk_sixteenths;
   a.want_large = want_large ? 1u : 0u;
   a.large_min_gap = min_gap;
   a.b_mode = c->tune.medium_mode;

@@ -45,12 +45,16 @@ constexpr int kAccCls143 = kAccCls28 + kCls28;              // 1650
 constexpr int kAccUsed = kAccCls143 + kCls143;              // 2794
 constexpr int kAccStride = 2800;
 
-// Shared-memory counter block (u32), same order as the accumulator from kAccHist on.
+// Shared-memory counter block (u32), same order as the accumulator from kAccHist on, except
+// that the class blocks are not wrapped: byte j of a word whose first byte has class c counts
+// in class c + j (up to 30 and 145), and the flush adds classes 28..30 / 143..145 to 0..2.
+constexpr int kSmCls28Rows = 28 + 3;
+constexpr int kSmCls143Rows = 143 + 3;
 constexpr int kSmHist = 0;
 constexpr int kSmModq = kSmHist + kHistBins;                // 1024
 constexpr int kSmCls28 = kSmModq + 8 * kModqBins;           // 1424
-constexpr int kSmCls143 = kSmCls28 + kCls28;                // 1648
-constexpr int kSmCounters = kSmCls143 + kCls143;            // 2792
+constexpr int kSmCls143 = kSmCls28 + 8 * kSmCls28Rows;      // 1672
+constexpr int kSmCounters = kSmCls143 + 8 * kSmCls143Rows;  // 2840
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 
@@ -116,6 +120,7 @@ struct SieveArgs {
   uint32_t chunk_words;     // odd; tile_words = blockDim.x * chunk_words
   uint32_t coop_div;
   uint32_t mult_factor;
+  uint32_t walk_sixteenths;
   uint32_t want_large;      // record large gaps
   uint32_t large_min_gap;   // 0: the reference's rule (gap >= 500 or merit >= 10); else every gap >= it
   uint32_t b_mode;          // medium primes: 0 = thread per prime, 1 = lane per (prime, residue)

@@ -113,14 +113,14 @@ __device__ __forceinline__ void clear_bit_word(uint32_t* bm, uint32_t word, uint
   atomicAnd(bm + word, mask);
 }
 
-// Clears bit `bit` of every byte start, start + 32p, start + 64p, ... below Lt (one lane of a
-// warp-cooperative small prime).  The stride is a multiple of 4 bytes, so the byte lane inside the
-// word, and with it the mask, never changes; four clears per loop trip.
-__device__ __forceinline__ void clear_lane_progression(uint32_t* bm, uint32_t start, uint32_t p,
+// Clears bit `bit` of every byte start, start + 4 ws, start + 8 ws, ... below Lt (one lane of a
+// warp-cooperative small prime; the stride is 4 ws bytes = ws words).  The stride is a multiple of
+// 4 bytes, so the byte lane inside the word, and with it the mask, never changes; four clears per
+// loop trip.
+__device__ __forceinline__ void clear_lane_progression(uint32_t* bm, uint32_t start, uint32_t ws,
                                                        uint32_t bit, uint32_t Lt, uint32_t nw,
                                                        uint32_t* err) {
   const uint32_t mask = ~(1u << (((start & 3u) << 3) | bit));
-  const uint32_t ws = 8u * p;                           // 32p bytes
   const uint32_t wlim = (Lt + 3u - (start & 3u)) >> 2;  // start + 4k < Lt  <=>  (start >> 2) + k < wlim
   uint32_t w = start >> 2;
   if (wlim > 3u * ws) {
@@ -223,7 +223,7 @@ __device__ unsigned long long g_phase_cycles[16];
 
 struct TileHdr {
   unsigned long long ktile, vbase, vlo, vhi, seg_k;
-  uint32_t nw, lt, np, ia, ib, iw, vb, gthr, k28, k143;
+  uint32_t nw, lt, np, ia, ib, iw, vb, cthr, k28, k143;
   uint32_t pre_base[kPreGroups];
   uint32_t interval, tile, next_tile, cur_iv, since_flush, flush;
   uint32_t r0, r1;       // base primes lying in the tile (restore)
@@ -350,6 +350,10 @@ __device__ __forceinline__ uint32_t acc_index(uint32_t i) {
   return (uint32_t)kAccCls143 + 8u * (c >= 143u ? c - 143u : c) + (i & 7u);
 }
 
+// Warp-cooperative primes p >= tile bytes / kSmallSplitDiv give each residue 4 lanes; smaller
+// ones give each residue all 32 lanes in turn.
+constexpr uint32_t kSmallSplitDiv = 512;
+
 constexpr uint32_t kFlushEvery = 2048;  // tiles between counter flushes (u32 headroom)
 
 template <int BLOCK, bool EMIT>
@@ -459,9 +463,14 @@ sieve_tiles_kernel(SieveArgs a) {
         if (kb < ktile + H.lt) vb = (uint32_t)(30ull * (kb - ktile));
       }
       H.vb = vb;
+      // large-gap candidates: g >= cthr, one tile-uniform threshold.  Reference rule
+      // (voss_v7_live.cu:289-294): g > 100 and (g >= 500 or g / log(p) >= 10); no gap of the tile
+      // below 10 log(vbase) - 2 can reach merit 10.  With large_min_gap: g >= large_min_gap.
       double lv = log((double)(H.vbase > 7 ? H.vbase : 7));
       double th = floor(10.0 * lv) - 2.0;
-      H.gthr = th < 0 ? 0u : (th > 1e9 ? 1000000000u : (uint32_t)th);
+      uint32_t gthr = th < 0 ? 0u : (th > 1e9 ? 1000000000u : (uint32_t)th);
+      gthr = gthr < 101u ? 101u : (gthr > 500u ? 500u : gthr);
+      H.cthr = !a.want_large ? kNone : (a.large_min_gap ? a.large_min_gap : gthr);
       H.k28 = (uint32_t)(ktile % 28ull);
       H.k143 = (uint32_t)(ktile % 143ull);
       const uint64_t wt = ktile >> 2;
@@ -511,6 +520,7 @@ sieve_tiles_kernel(SieveArgs a) {
       const uint64_t ktile = H.ktile;
       const uint32_t ia = H.ia, ib = H.ib, iw = H.iw, np = H.np;
       // small primes: a warp per prime
+      const uint32_t split = Lt / kSmallSplitDiv;
       for (;;) {
         uint32_t i = 0;
         if (lane == 0) i = atomicAdd(&H.coop_ctr, 1u);
@@ -519,12 +529,22 @@ sieve_tiles_kernel(SieveArgs a) {
         const uint32_t p = a.primes[i];
         const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
         const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
-#pragma unroll 1
-        for (uint32_t o = 0; o < 8; ++o) {
+        if (p >= split) {
+          // 4 lanes per residue progression (lane = 4 o + q: bytes s_o + q p + 4p k)
+          const uint32_t o = (uint32_t)lane >> 2;
           const uint32_t e = s_step[bi * 8u + o];
           const uint32_t delta = pa * w30(o) + (e & 31u);
           const uint32_t s = delta >= r ? delta - r : delta + p - r;
-          clear_lane_progression(bm, s + (uint32_t)lane * p, p, e >> 5, Lt, nw, err);
+          clear_lane_progression(bm, s + ((uint32_t)lane & 3u) * p, p, e >> 5, Lt, nw, err);
+        } else {
+          // all 32 lanes on one residue progression, residues in turn (lane q: bytes s_o + q p + 32p k)
+#pragma unroll 1
+          for (uint32_t o = 0; o < 8; ++o) {
+            const uint32_t e = s_step[bi * 8u + o];
+            const uint32_t delta = pa * w30(o) + (e & 31u);
+            const uint32_t s = delta >= r ? delta - r : delta + p - r;
+            clear_lane_progression(bm, s + (uint32_t)lane * p, 8u * p, e >> 5, Lt, nw, err);
+          }
         }
       }
       VOSS_PHASE(3)
@@ -662,7 +682,7 @@ sieve_tiles_kernel(SieveArgs a) {
       // without wrapping (k mod 28 + j up to 30, k mod 143 + j up to 145: 31 and 146 classes);
       // the flush folds the tail classes back.  That makes both class indices one add per prime.
       const uint32_t vb = H.vb;
-      const uint32_t gthr = H.gthr;
+      const uint32_t cthr = H.cthr;
       uint32_t c28 = (uint32_t)kSmCls28 + 8u * ((H.k28 + 4u * c0) % 28u);
       uint32_t c143 = (uint32_t)kSmCls143 + 8u * ((H.k143 + 4u * c0) % 143u);
       uint32_t my_cnt = 0, mg = 0, mlo = 0;
@@ -706,8 +726,7 @@ sieve_tiles_kernel(SieveArgs a) {
           }
           mlo = g > mg ? (uint32_t)prev : mlo;
           mg = g > mg ? g : mg;
-          const bool cand = a.large_min_gap ? (g >= a.large_min_gap) : (g > 100u && (g >= 500u || g >= gthr));
-          if (a.want_large && cand && !crossing) {
+          if (g >= cthr && !crossing) {
             const uint64_t v0 = H.vbase + (uint32_t)prev;
             const double merit_d = (double)g / log((double)v0);
             if (a.large_min_gap || g >= 500u || merit_d >= 10.0) {

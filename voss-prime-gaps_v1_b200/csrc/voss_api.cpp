@@ -240,11 +240,24 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
   bool scatter = P.n_tiles && j1 > j0 && p_large <= 0xFFFFFFFFull && gbm_bytes <= W.gbm_budget &&
                  (!W.gbm_fixed || gbm_bytes <= W.gbm.bytes);
   std::vector<IntervalScatter> sc;
+  // Windows of consecutive intervals whose bitmap words total at most kScatterWindowBytes: the
+  // pre-pass runs window by window, so that its atomics find their lines in L2 (the bitmap of a
+  // whole launch can be gigabytes).  Inside a window, intervals are sorted by isqrt(hi)
+  // descending (the kernel stops a prime at the first interval it does not reach).
+  struct Window {
+    uint32_t off, n, j1;
+  };
+  std::vector<Window> wins;
   if (scatter) {
+    uint64_t wbytes = 0;
     for (const IntervalDev& d : P.iv) {
       if (!d.n_tiles) continue;
       const uint64_t sq = isqrt_u64(d.hi - 1);
       if (sq < p_large) continue;
+      if (wins.empty() || (wbytes && wbytes + 4ull * d.n_words > kScatterWindowBytes)) {
+        wins.push_back(Window{(uint32_t)sc.size(), 0, j0});
+        wbytes = 0;
+      }
       IntervalScatter I;
       I.vbase = 30ull * d.k0;
       I.span = 120ull * d.n_words;
@@ -252,8 +265,14 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
       I.sqrt_hi = (uint32_t)std::min<uint64_t>(sq, 0xFFFFFFFFull);
       I.pad = 0;
       sc.push_back(I);
+      wbytes += 4ull * d.n_words;
+      wins.back().n++;
     }
-    std::sort(sc.begin(), sc.end(), [](const IntervalScatter& x, const IntervalScatter& y) { return x.sqrt_hi > y.sqrt_hi; });
+    for (Window& w : wins) {
+      std::sort(sc.begin() + w.off, sc.begin() + w.off + w.n,
+                [](const IntervalScatter& x, const IntervalScatter& y) { return x.sqrt_hi > y.sqrt_hi; });
+      w.j1 = (uint32_t)(std::upper_bound(c->primes.begin(), c->primes.end(), sc[w.off].sqrt_hi) - c->primes.begin());
+    }
     if ((rc = W.gbm.ensure(gbm_bytes)) || (rc = W.scat.ensure(sizeof(IntervalScatter) * sc.size()))) return rc;
     CUDA_TRY(cudaMemsetAsync(W.gbm.p, 0xFF, gbm_bytes, s));
     CUDA_TRY(cudaMemcpyAsync(W.scat.p, sc.data(), sizeof(IntervalScatter) * sc.size(), cudaMemcpyHostToDevice, s));
@@ -261,9 +280,10 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
     a.scatter_first = j0;
   }
   CUDA_TRY(cudaEventRecord(E.ev0, s));
-  if (scatter && launch_scatter_large(a.primes, a.magic, j0, j1, W.scat.as<IntervalScatter>(), (uint32_t)sc.size(),
-                                      W.gbm.as<uint32_t>(), c->sm_count, s))
-    return fail(VOSS_ERR_CUDA, "large-prime pre-pass launch failed");
+  for (const Window& w : wins)
+    if (launch_scatter_large(a.primes, a.magic, j0, w.j1, W.scat.as<IntervalScatter>() + w.off, w.n,
+                             W.gbm.as<uint32_t>(), c->sm_count, s))
+      return fail(VOSS_ERR_CUDA, "large-prime pre-pass launch failed");
   if (P.n_tiles) {
     int lr = emit ? launch_sieve_emit(a, grid, (int)c->tune.block_threads, smem, s)
                   : launch_sieve_stats(a, grid, (int)c->tune.block_threads, smem, s);

@@ -66,6 +66,9 @@ enum { kCtrTile = 0, kCtrLarge = 1, kCtrOver = 2, kCtrError = 3, kCtrMrWork = 4,
 constexpr uint64_t kMaxHi = 1ull << 62;
 constexpr uint32_t kOverCap = 1u << 16;
 constexpr uint64_t kDefaultLargeCap = 1ull << 22;
+// Large-prime pre-pass windows: bitmap bytes per window, well inside the 126 MB L2 next to the
+// base-prime table (69 MB for primes below 10^8).
+constexpr uint64_t kScatterWindowBytes = 32ull << 20;
 constexpr uint64_t kMaxLargeCap = 50000000ull;  // MAX_LARGE_GAPS, src/voss_v7_live.cu:34
 
 }  // namespace voss_host

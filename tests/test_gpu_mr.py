@@ -58,3 +58,28 @@ def test_prove_gaps(gpu_ctx):
     want = O.ref_prove_gaps(P, G) if __import__("os").path.exists(O.REF_VERIFY_SO) else O.prove_gaps(P, G)
     np.testing.assert_array_equal(got, want)
     assert got[: p.size].all()
+
+
+def test_prove_gaps_long_joined_and_high(gpu_ctx):
+    """Proofs that span several 256-integer rounds (the maximal gap below 1e12, found by the
+    sieve), joined gaps whose interior holds a prime, and endpoints just below 2^64."""
+    checker = O.ref_prove_gaps if __import__("os").path.exists(O.REF_VERIFY_SO) else O.prove_gaps
+    big = gpu_ctx.gaps_at_least(7 * 10**11, 8 * 10**11, 500)
+    assert big.size and int(big["gap"].max()) >= 514
+    ps = gpu_ctx.primes_range(10**11, 10**11 + 20000)
+    joined_p = ps[2:200]
+    joined_g = (ps[2:200] - ps[:198]).astype(np.int32)  # interior holds ps[1:199]
+    odd = np.uint64(2**64 - 3001) + np.arange(0, 3000, 2, dtype=np.uint64)
+    top = odd[gpu_ctx.mr_verify(odd).astype(bool)]
+    assert top.size >= 3
+    top_p, top_g = top[1:], (top[1:] - top[:-1]).astype(np.int32)
+    P = np.concatenate([big["position"].astype(np.uint64), joined_p, top_p, top_p[:1]])
+    G = np.concatenate([big["gap"].astype(np.int32), joined_g, top_g, 2 * top_g[:1]])  # last: holds top[0] or starts at a composite
+    got = gpu_ctx.prove_gaps(P, G)
+    nb, nj = big.size, joined_p.size
+    # the reference checker sieves with every prime below isqrt(p_after): affordable below 1e12;
+    # near 2^64 every odd integer of the window was tested above, so consecutive entries of
+    # `top` are consecutive primes and their proofs must hold
+    np.testing.assert_array_equal(got[:nb + nj], checker(P[:nb + nj], G[:nb + nj]))
+    assert got[:nb].all() and not got[nb:nb + nj].any()
+    assert got[nb + nj:-1].all() and not got[-1]

@@ -54,6 +54,21 @@ __device__ __forceinline__ uint64_t mod_add(uint64_t a, uint64_t b, uint64_t n) 
   return (s < a || s >= n) ? s - n : s;
 }
 
+// 2^64 mod n for odd n > 1.  For n >= 2^32 the quotient q* = floor(2^64 / n), 1 <= q* < 2^32,
+// is estimated in double precision (relative error < 2^-51, so the estimate is off by at most 1)
+// and lowered by one, but not below 1: then q* - 2 <= q <= q* and q >= 1, so 2^64 - q n is below
+// 2^64, lies in [0, 3n), and at most two subtractions finish it.  Smaller n take the 64-bit
+// integer remainder.
+__device__ __forceinline__ uint64_t two64_mod(uint64_t n) {
+  if (n < (1ull << 32)) return (0ull - n) % n;
+  uint64_t q = (uint64_t)(18446744073709551616.0 / (double)n);
+  q = q > 1 ? q - 1 : 1;
+  uint64_t r = 0ull - q * n;  // 2^64 - q n
+  if (r >= n) r -= n;
+  if (r >= n) r -= n;
+  return r;
+}
+
 __device__ __forceinline__ Mont mont_setup(uint64_t n) {
   Mont M;
   M.n = n;
@@ -61,7 +76,7 @@ __device__ __forceinline__ Mont mont_setup(uint64_t n) {
 #pragma unroll
   for (int i = 0; i < 5; ++i) x *= 2ull - n * x;
   M.ninv = 0ull - x;
-  M.one = (0ull - n) % n;  // 2^64 mod n
+  M.one = two64_mod(n);  // R mod n
   M.mone = n - M.one;
   return M;
 }
@@ -240,37 +255,81 @@ __device__ __forceinline__ uint64_t isqrt64(uint64_t x) {
   return s;
 }
 
-__global__ void prove_gaps_kernel(const uint64_t* __restrict__ p_after, const int32_t* __restrict__ gap,
-                                  uint64_t count, uint8_t* __restrict__ ok) {
-  const int lane = threadIdx.x & 31;
+// Endpoints of every gap, [2g] = p_after - gap (as the reference: u64 wrap-around), [2g+1] = p_after.
+__global__ void gap_ends_kernel(const uint64_t* __restrict__ p_after, const int32_t* __restrict__ gap,
+                                uint64_t count, uint64_t* __restrict__ ends) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < count; g += stride) {
+    const uint64_t pa = p_after[g];
+    ends[2 * g] = pa - (uint64_t)(int64_t)gap[g];
+    ends[2 * g + 1] = pa;
+  }
+}
+
+constexpr int kProveBlock = 256;
+constexpr uint32_t kProveChunk = 256;  // interior odd integers examined per round (list capacity)
+
+// Interior proofs, one warp per gap, after the endpoints have been tested (end_ok).  Per round of
+// kProveChunk odd interior integers: trial division by the bases 3..37 on all lanes, the
+// undecided integers above isqrt(p_after) are appended to a per-warp list in shared memory, and
+// the list is tested 32 at a time by a warp-uniform base-2 strong probable-prime test; only
+// integers passing it (primes, or base-2 strong pseudoprimes) take the remaining bases.
+__global__ void __launch_bounds__(kProveBlock) prove_interior_kernel(const uint64_t* __restrict__ p_after,
+                                                                     const int32_t* __restrict__ gap, uint64_t count,
+                                                                     const uint8_t* __restrict__ end_ok,
+                                                                     uint8_t* __restrict__ ok) {
+  __shared__ uint64_t s_list[kProveBlock / 32][kProveChunk];
+  const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  uint64_t* list = s_list[wib];
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < count; g += warps) {
+  for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib; g < count; g += warps) {
     const uint64_t pa = p_after[g];
     const int32_t gp = gap[g];
     const uint64_t pb = pa - (uint64_t)(int64_t)gp;
-    bool end_ok = true;
-    if (lane == 0) end_ok = is_prime_u64_dev(pb);
-    if (lane == 1) end_ok = is_prime_u64_dev(pa);
-    const bool ends = __all_sync(0xFFFFFFFFu, end_ok);
-    bool res = ends;
-    if (ends && gp >= 2) {
+    bool res = end_ok[2 * g] && end_ok[2 * g + 1];
+    if (res && gp >= 2) {
       if ((pb & 1ull) == 0) {
         res = false;  // p_before = 2: the even-index marking leaves interior 4 unmarked
       } else {
         const uint64_t sq = isqrt64(pa);
         const uint64_t n_odd = (uint64_t)(gp - 2) / 2;  // odd integers pb+2 .. pa-2
         bool bad = false;
-        for (uint64_t k0 = 0; k0 < n_odd; k0 += 32) {
-          const uint64_t k = k0 + lane;
-          bool unmarked = false;
-          if (k < n_odd) {
-            const uint64_t v = pb + 2 + 2 * k;
-            if (v > sq) unmarked = is_prime_u64_dev(v);
+        for (uint64_t k0 = 0; k0 < n_odd && !bad; k0 += kProveChunk) {
+          const uint64_t k1 = n_odd - k0 < kProveChunk ? n_odd : k0 + kProveChunk;
+          uint32_t n_list = 0;
+          bool small_prime = false;
+          for (uint64_t kb = k0; kb < k1; kb += 32) {  // warp-uniform trip count
+            const uint64_t k = kb + lane;
+            int t = 0;
+            uint64_t v = 0;
+            if (k < k1) {
+              v = pb + 2 + 2 * k;
+              if (v > sq) t = trial_phase(v);  // 1: a base prime, 0: has a factor <= 37, -1: undecided
+            }
+            small_prime |= (t == 1);
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, t < 0);
+            if (t < 0) list[n_list + (uint32_t)__popc(m & ((1u << lane) - 1u))] = v;
+            n_list += (uint32_t)__popc(m);
           }
-          if (__any_sync(0xFFFFFFFFu, unmarked)) {
-            bad = true;
-            break;
+          __syncwarp();
+          bad = __any_sync(0xFFFFFFFFu, small_prime);
+          for (uint32_t b0 = 0; b0 < n_list && !bad; b0 += 32) {
+            const bool live = b0 + lane < n_list;
+            const uint64_t v = list[live ? b0 + lane : b0];  // idle lanes shadow the first entry
+            const Mont M = mont_setup(v);
+            uint64_t d = v - 1;
+            const int r = __ffsll((long long)d) - 1;
+            d >>= r;
+            const int top = 63 - __clzll(d);
+            const int top_w = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)top);
+            const int r_w = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)r);
+            const bool pass = live && sprp_uniform(M, 0, d, r, top_w, r_w, true);
+            if (__any_sync(0xFFFFFFFFu, pass)) {
+              const bool prime = pass && sprp_rest(M, d, r);
+              bad = __any_sync(0xFFFFFFFFu, prime);
+            }
           }
+          __syncwarp();
         }
         res = !bad;
       }
@@ -317,15 +376,22 @@ int launch_mr(const uint64_t* d_n, uint64_t count, uint8_t* d_out, uint32_t* d_w
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
-int launch_prove_gaps(const uint64_t* d_p_after, const int32_t* d_gap, uint64_t count,
-                      uint8_t* d_ok, void* stream, int sm_count) {
+int launch_prove_gaps(const uint64_t* d_p_after, const int32_t* d_gap, uint64_t count, uint8_t* d_ok,
+                      uint64_t* d_ends, uint8_t* d_ends_ok, uint32_t* d_work, uint32_t* d_nwork, void* stream,
+                      int sm_count) {
   if (ensure_mr_tables()) return -1;
   if (count == 0) return 0;
-  const int blk = 256;
-  const uint64_t warps_needed = count;
-  uint64_t want = (warps_needed + (blk / 32) - 1) / (blk / 32);
-  int grid = (int)(want < (uint64_t)sm_count * 16 ? want : (uint64_t)sm_count * 16);
-  prove_gaps_kernel<<<grid, blk, 0, (cudaStream_t)stream>>>(d_p_after, d_gap, count, d_ok);
+  if (count > 0x7FFFFFFFull) return -1;
+  cudaStream_t s = (cudaStream_t)stream;
+  // 1. both endpoints of every gap through the batched Miller-Rabin kernels
+  const uint64_t eg = (count + 255) / 256;
+  gap_ends_kernel<<<(int)(eg < (uint64_t)sm_count * 8 ? eg : (uint64_t)sm_count * 8), 256, 0, s>>>(d_p_after, d_gap,
+                                                                                                   count, d_ends);
+  if (launch_mr(d_ends, 2 * count, d_ends_ok, d_work, d_nwork, stream, sm_count)) return -1;
+  // 2. interiors
+  const uint64_t want = (count + (kProveBlock / 32) - 1) / (kProveBlock / 32);
+  const int grid = (int)(want < (uint64_t)sm_count * 8 ? want : (uint64_t)sm_count * 8);
+  prove_interior_kernel<<<grid, kProveBlock, 0, s>>>(d_p_after, d_gap, count, d_ends_ok, d_ok);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

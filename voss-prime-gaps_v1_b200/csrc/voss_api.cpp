@@ -814,16 +814,22 @@ VOSS_API int voss_prove_gaps(voss_ctx* c, const uint64_t* p_after, const int32_t
   if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
   if (count == 0) return VOSS_OK;
   if (!p_after || !gap || !ok) return fail(VOSS_ERR_ARG, "NULL argument");
+  if (count > 0x7FFFFFFFull) return fail(VOSS_ERR_ARG, "count must be < 2^31 per call");
   cudaSetDevice(c->device);
   cudaStream_t s = c->stream;
-  DevBuf dp, dg, dok;
+  Workspace& W = c->ws;  // context-owned, grow-only buffers: repeated calls do not allocate
   int rc;
-  if ((rc = dp.ensure(count * 8)) || (rc = dg.ensure(count * 4)) || (rc = dok.ensure(count))) return rc;
-  CUDA_TRY(cudaMemcpyAsync(dp.p, p_after, count * 8, cudaMemcpyHostToDevice, s));
-  CUDA_TRY(cudaMemcpyAsync(dg.p, gap, count * 4, cudaMemcpyHostToDevice, s));
-  if (launch_prove_gaps(dp.as<uint64_t>(), dg.as<int32_t>(), count, dok.as<uint8_t>(), s, c->sm_count))
+  if ((rc = W.pg_pa.ensure(count * 8)) || (rc = W.pg_gap.ensure(count * 4)) || (rc = W.pg_ok.ensure(count)) ||
+      (rc = W.mr_in.ensure(2 * count * 8)) || (rc = W.mr_out.ensure(2 * count)) ||
+      (rc = W.mr_work.ensure(sizeof(uint32_t) * (2 * count + 8))))
+    return rc;
+  CUDA_TRY(cudaMemcpyAsync(W.pg_pa.p, p_after, count * 8, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(W.pg_gap.p, gap, count * 4, cudaMemcpyHostToDevice, s));
+  uint32_t* work = W.mr_work.as<uint32_t>();
+  if (launch_prove_gaps(W.pg_pa.as<uint64_t>(), W.pg_gap.as<int32_t>(), count, W.pg_ok.as<uint8_t>(),
+                        W.mr_in.as<uint64_t>(), W.mr_out.as<uint8_t>(), work + 8, work, s, c->sm_count))
     return fail(VOSS_ERR_CUDA, "gap proof launch failed");
-  CUDA_TRY(cudaMemcpyAsync(ok, dok.p, count, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(ok, W.pg_ok.p, count, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   return VOSS_OK;
 }

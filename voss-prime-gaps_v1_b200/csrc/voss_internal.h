@@ -167,7 +167,10 @@ int probe_smem_rmw(int sm_count, void* stream, float* ms, double* bytes);
 // Miller-Rabin (mr_kernels.cu).
 int launch_mr(const uint64_t* d_n, uint64_t count, uint8_t* d_out, uint32_t* d_work,
               uint32_t* d_nwork, void* stream, int sm_count);
-int launch_prove_gaps(const uint64_t* d_p_after, const int32_t* d_gap, uint64_t count,
-                      uint8_t* d_ok, void* stream, int sm_count);
+// Gap proofs: endpoints (into d_ends / d_ends_ok, 2 * count each) through the Miller-Rabin
+// kernels (work list d_work, counter d_nwork), then the interiors; count < 2^31.
+int launch_prove_gaps(const uint64_t* d_p_after, const int32_t* d_gap, uint64_t count, uint8_t* d_ok,
+                      uint64_t* d_ends, uint8_t* d_ends_ok, uint32_t* d_work, uint32_t* d_nwork, void* stream,
+                      int sm_count);
 
 }  // namespace voss

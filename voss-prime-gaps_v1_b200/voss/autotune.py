@@ -14,14 +14,16 @@ import time
 
 import numpy as np
 
-# candidate tunings: tile bytes from 200 KB (1 CTA/SM) down to 14 KB (many CTAs/SM)
+# candidate tunings: tile bytes from 200 KB (1 CTA/SM) down to 36 KB (several CTAs/SM), with the
+# small/medium split (coop_div) and the pre-pass threshold (mult_factor) near their measured optima
 CANDIDATES = [
-    dict(block_threads=1024, chunk_words=49, coop_div=48, mult_factor=8),
-    dict(block_threads=1024, chunk_words=25, coop_div=48, mult_factor=8),
-    dict(block_threads=512, chunk_words=45, coop_div=32, mult_factor=8),
+    dict(block_threads=1024, chunk_words=49, coop_div=128, mult_factor=8),
+    dict(block_threads=1024, chunk_words=49, coop_div=64, mult_factor=8),
+    dict(block_threads=1024, chunk_words=49, coop_div=64, mult_factor=16),
+    dict(block_threads=1024, chunk_words=25, coop_div=64, mult_factor=8),
+    dict(block_threads=512, chunk_words=45, coop_div=64, mult_factor=8),
     dict(block_threads=512, chunk_words=21, coop_div=32, mult_factor=8),
     dict(block_threads=512, chunk_words=9, coop_div=16, mult_factor=4),
-    dict(block_threads=512, chunk_words=3, coop_div=8, mult_factor=2),
 ]
 
 CLASS_EDGES = (10**5, 10**6, 10**7)  # interval lengths: tiny / small / medium / large

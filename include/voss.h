@@ -209,6 +209,14 @@ VOSS_API int voss_mr_verify_noalloc(const uint64_t* d_n, uint64_t count, uint8_t
 VOSS_API int voss_prove_gaps(voss_ctx* ctx, const uint64_t* p_after, const int32_t* gap,
                              uint64_t count, uint8_t* ok);
 
+/* SHA-256 of count messages at once (the digest step of the gap certificates,
+ * scripts/generate_certificates.py:105-108, which hashes "VOSS|p_before|p_after|gap|merit:.6f"
+ * with hashlib one string at a time).  Message i is data[offsets[i] .. offsets[i+1]);
+ * offsets has count + 1 entries, offsets[0] = 0, non-decreasing.  digests receives 32 bytes
+ * per message (the FIPS 180-4 digest, big-endian words).  Host buffers. */
+VOSS_API int voss_sha256_batch(voss_ctx* ctx, const uint8_t* data, const uint64_t* offsets,
+                               uint64_t count, uint8_t* digests);
+
 /* ---- artifacts --------------------------------------------------------------- */
 /* Write gap_histogram.csv, hl_trend.csv, modq_counts.csv, modq_gap_hist.csv,
  * chebyshev.csv and large_gaps.csv into `dir` in the byte format of

@@ -44,6 +44,7 @@ struct Workspace {
   DevBuf iv, partials, acc, out, large, large_iv, over, counters, istats, offsets, emit, mr_work, mr_in, mr_out;
   DevBuf gbm, scat;  // large-prime pre-pass: bitmap of the launch and its interval descriptors
   DevBuf pg_pa, pg_gap, pg_ok;  // gap proofs: inputs and verdicts (endpoints use mr_in / mr_out / mr_work)
+  DevBuf sha_data, sha_off, sha_out;  // certificate hashing: messages, offsets, digests
   // Largest large-prime bitmap this workspace may use; with gbm_fixed the buffers are never
   // grown (server slots size them at creation), and launches that need more skip the pre-pass.
   size_t gbm_budget = 8ull << 30;

@@ -110,6 +110,7 @@ SIGNATURES = {
     "voss_mr_verify_device": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p]),
     "voss_mr_verify_noalloc": (c_int, [c_void_p, c_uint64, c_void_p, c_void_p]),
     "voss_prove_gaps": (c_int, [c_void_p, POINTER(c_uint64), POINTER(c_int32), c_uint64, POINTER(c_uint8)]),
+    "voss_sha256_batch": (c_int, [c_void_p, POINTER(c_uint8), POINTER(c_uint64), c_uint64, POINTER(c_uint8)]),
     "voss_write_artifacts": (c_int, [POINTER(RangeStats), POINTER(LargeGap), c_uint64, c_char_p]),
     "voss_stats_merge": (c_int, [POINTER(RangeStats), c_uint32, POINTER(RangeStats), POINTER(LargeGap),
                                  c_uint64, c_uint64, POINTER(c_uint64)]),

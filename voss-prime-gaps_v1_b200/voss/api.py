@@ -224,6 +224,19 @@ class Context:
                                          p.size, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
         return out
 
+    def sha256_batch(self, messages) -> np.ndarray:
+        """SHA-256 digests of a list of byte strings on the GPU, as a (len, 32) uint8 array."""
+        msgs = [bytes(m) for m in messages]
+        off = np.zeros(len(msgs) + 1, dtype=np.uint64)
+        if msgs:
+            off[1:] = np.cumsum([len(m) for m in msgs], dtype=np.uint64)
+        data = np.frombuffer(b"".join(msgs), dtype=np.uint8) if off[-1] else np.zeros(1, dtype=np.uint8)
+        out = np.zeros((len(msgs), 32), dtype=np.uint8)
+        if msgs:
+            N.check(self.lib.voss_sha256_batch(self._h, data.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), _u64p(off),
+                                               len(msgs), out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+        return out
+
     def probe_smem_rmw(self) -> float:
         g = c_double()
         N.check(self.lib.voss_probe_smem_rmw(self._h, byref(g)))

@@ -213,6 +213,10 @@ def ref_cuda_baseline(n: int) -> dict | None:
 
 
 # ---------------------------------------------------------------------------------------
+def range_workload(n: int) -> str:
+    return f"wheel-30 sieve + reference statistics of [1, {n}] per GPU (REF_COMPAT, SEG_NUM={SEG_NUM})"
+
+
 def run_reference_arm(a) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -240,8 +244,9 @@ def run_reference_arm(a) -> None:
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "range/s", "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic (integer range)",
-        "config": {"workload": f"sieve+stats of [1, {a.n}] (bounded CPU sample)", "n": a.n, "seg_num": SEG_NUM},
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (the integer range itself)",
+        "config": {"workload": range_workload(a.n), "n_per_gpu": a.n, "range": [1, a.n],
+                   "parallelism": f"host CPU, {threads} threads (rank 0 only)"},
         "cpu_baseline": {"value": value, "unit": "range/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "range/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -566,8 +571,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "range/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (the integer range itself)",
-        "config": {"workload": f"wheel-30 sieve + reference statistics of [1, {n}] per GPU "
-                               f"(REF_COMPAT, SEG_NUM={SEG_NUM})", "n_per_gpu": n,
+        "config": {"workload": range_workload(n), "n_per_gpu": n,
                    "range": [1, total_range], "l2": "flushed (256 MiB write) between timed steps",
                    "tuning": ctx.tuning(), "parallelism": f"range-sharded x{world}"},
         "e2e": {"value": total_range / e2e_s, "unit": "range/s", "h2d_bytes_per_step": 48,

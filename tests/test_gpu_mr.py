@@ -9,7 +9,9 @@ pytestmark = pytest.mark.gpu
 
 SPECIAL = [0, 1, 2, 3, 4, 5, 9, 25, 37, 41, 43, 1369, 2047, 3215031751, 341550071728321,
            3825123056546413051, 18446744073709551557, 18446744073709551615, 18446744073709551614,
-           2**61 - 1, 2**63 - 25, 2**64 - 59, 1000000007, 999999999989, 4759123141, 1122004669633]
+           2**61 - 1, 2**63 - 25, 2**64 - 59, 1000000007, 999999999989, 4759123141, 1122004669633,
+           # smallest strong pseudoprimes to the first 2, 3, 5, 6 prime bases (OEIS A014233)
+           1373653, 25326001, 2152302898747, 3474749660383, 3474749660383 + 2, 341550071728321 - 2]
 
 
 def checker(n):
@@ -41,6 +43,20 @@ def test_mr_strong_pseudoprimes(gpu_ctx):
     a = rng.choice(q, 5000)
     b = 2 * a - 1
     n = (a * b).astype(np.uint64)
+    np.testing.assert_array_equal(gpu_ctx.mr_verify(n), checker(n))
+
+
+def test_mr_bands_of_base_counts(gpu_ctx):
+    """Random odd values in each band where a different number of bases is exact (below
+    3,474,749,660,383: 6; below 341,550,071,728,321: 7; below 3,825,123,056,546,413,051: 9;
+    above: 12), the bands' edges, and sieved primes on both sides of the first edge."""
+    rng = np.random.default_rng(77)
+    edges = [3474749660383, 341550071728321, 3825123056546413051]
+    lo_hi = [(10**6, edges[0]), (edges[0], edges[1]), (edges[1], edges[2]), (edges[2], 2**64 - 1)]
+    parts = [(rng.integers(a // 2, b // 2, 100_000, dtype=np.uint64) * 2 + 1) for a, b in lo_hi]
+    parts.append(np.array([e + d for e in edges for d in range(-41, 42, 2)], dtype=np.uint64))
+    parts.append(gpu_ctx.primes_range(edges[0] - 3 * 10**5, edges[0] + 3 * 10**5))
+    n = np.concatenate(parts)
     np.testing.assert_array_equal(gpu_ctx.mr_verify(n), checker(n))
 
 

@@ -11,7 +11,9 @@
 // Base 2 is special-cased: its square-and-multiply multiplies by 2 with a modular addition.
 // Work is split in two kernels so that warps stay full: mr_sieve_kernel resolves every
 // candidate that trial division or base 2 decides (nearly all composites) and appends the rest
-// to a work list; mr_finish_kernel runs the remaining eleven bases on that list.
+// to a work list; mr_finish_kernel runs the remaining bases on that list, as many as the size
+// of n requires for an exact verdict (bases_needed: 6, 7, 9 or all 12), so its results equal
+// the reference's twelve-base test for every 64-bit n.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -96,6 +98,16 @@ __device__ __forceinline__ int trial_phase(uint64_t n) {
   return -1;
 }
 
+// How many of the bases 2, 3, 5, ..., 37 (in this order) decide primality exactly for n.  The
+// smallest strong pseudoprimes to the first k prime bases are 3,474,749,660,383 (k = 6),
+// 341,550,071,728,321 (k = 7, 8) and 3,825,123,056,546,413,051 (k = 9..11) (Jaeschke 1993; OEIS
+// A014233); below them the first 6, 7 or 9 bases already give the same verdict as all twelve,
+// which remain exact for every n < 2^64.
+__device__ __forceinline__ int bases_needed(uint64_t n) {
+  return n < 3474749660383ull ? 6 : (n < 341550071728321ull ? 7 : (n < 3825123056546413051ull ? 9 : 12));
+}
+constexpr uint64_t kSmallMr = 3474749660383ull;  // survivors below go to the front work list
+
 // Strong probable-prime test of odd n > 37 to the base whose Montgomery form is am.
 __device__ __forceinline__ bool sprp(const Mont& M, uint64_t am, uint64_t d, int r) {
   uint64_t x = M.one;
@@ -177,13 +189,23 @@ __global__ void mr_sieve_kernel(const uint64_t* __restrict__ cand, uint64_t coun
       }
     }
     __syncwarp();
-    const unsigned mask = __ballot_sync(0xFFFFFFFFu, need);
-    if (mask) {
+    // survivors below kSmallMr (6 bases) fill the work list from the front, the others from the
+    // back, so that the warps of mr_finish_kernel mostly share one base count
+    const bool small = need && cand[i] < kSmallMr;
+    const unsigned ms = __ballot_sync(0xFFFFFFFFu, small);
+    const unsigned ml = __ballot_sync(0xFFFFFFFFu, need && !small);
+    if (ms | ml) {
       const int lane = threadIdx.x & 31;
-      uint32_t slot = 0;
-      if (lane == 0) slot = atomicAdd(nwork, (uint32_t)__popc(mask));
-      slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-      if (need) work[slot + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)i;
+      uint32_t s0 = 0, s1 = 0;
+      if (lane == 0) {
+        if (ms) s0 = atomicAdd(nwork, (uint32_t)__popc(ms));
+        if (ml) s1 = atomicAdd(nwork + 1, (uint32_t)__popc(ml));
+      }
+      s0 = __shfl_sync(0xFFFFFFFFu, s0, 0);
+      s1 = __shfl_sync(0xFFFFFFFFu, s1, 0);
+      const unsigned below = (1u << lane) - 1u;
+      if (small) work[s0 + __popc(ms & below)] = (uint32_t)i;
+      else if (need) work[count - 1 - (s1 + __popc(ml & below))] = (uint32_t)i;
     }
   }
 }
@@ -208,17 +230,20 @@ __device__ __forceinline__ bool sprp_uniform(const Mont& M, uint64_t am, uint64_
   return ok;
 }
 
-// `work` holds candidate indices (< 2^32: the entry points take fewer than 2^32 candidates per call).
+// `work` holds candidate indices (< 2^32: the entry points take fewer than 2^32 candidates per call):
+// nwork[0] of them at the front, nwork[1] at the back (work[count - 1], work[count - 2], ...).
 __global__ void mr_finish_kernel(const uint64_t* __restrict__ cand, uint8_t* __restrict__ out,
-                                 const uint32_t* __restrict__ work, const uint32_t* __restrict__ nwork) {
-  const uint32_t nw = *nwork;
+                                 const uint32_t* __restrict__ work, const uint32_t* __restrict__ nwork,
+                                 uint32_t count) {
+  const uint32_t na = nwork[0];
+  const uint32_t nw = na + nwork[1];
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t base = warp0 * 32u; base < nw; base += nwarps * 32u) {  // warp-uniform loop
     const uint32_t k = base + lane;
     const bool live = k < nw;
-    const uint32_t i = live ? work[k] : 0u;
+    const uint32_t i = live ? work[k < na ? k : count - 1 - (k - na)] : 0u;
     uint64_t n = live ? cand[i] : 0ull;
     const uint64_t n0 = __shfl_sync(0xFFFFFFFFu, n, 0);  // idle lanes shadow lane 0
     if (!live) n = n0;
@@ -232,13 +257,17 @@ __global__ void mr_finish_kernel(const uint64_t* __restrict__ cand, uint8_t* __r
     const uint64_t n_ = M.n;
     const uint64_t r1 = M.one, r2 = mod_add(r1, r1, n_), r4 = mod_add(r2, r2, n_), r6 = mod_add(r4, r2, n_);
     uint64_t a = mod_add(r2, r1, n_);  // 3R: bases 3,5,7,11,13,17,19,23,29,31,37 by their gaps
+    const int need = bases_needed(n);  // >= 6: bases 2 (done) and 3 always run
     bool prime = sprp_uniform(M, a, d, r, top_w, r_w, false);
 #pragma unroll 1
     for (int s = 0; s < 10; ++s) {
-      if (!__any_sync(0xFFFFFFFFu, prime)) break;  // every lane already composite
+      // base index s + 2 (5, 7, 11, ...): still wanted by a lane that is prime so far and needs it
+      const bool want = prime && (s + 2 < need);
+      if (!__any_sync(0xFFFFFFFFu, want)) break;
       const int step = (0x6264242422ull >> (4 * s)) & 0xF;  // 2,2,4,2,4,2,4,6,2,6
       a = mod_add(a, step == 2 ? r2 : (step == 4 ? r4 : r6), n_);
-      prime &= sprp_uniform(M, a, d, r, top_w, r_w, false);
+      const bool pass = sprp_uniform(M, a, d, r, top_w, r_w, false);
+      prime = want ? pass : prime;
     }
     if (live) out[i] = prime ? 1 : 0;
   }
@@ -367,12 +396,12 @@ int launch_mr(const uint64_t* d_n, uint64_t count, uint8_t* d_out, uint32_t* d_w
   if (count == 0) return 0;
   if (count > 0xFFFFFFFFull) return -1;
   cudaStream_t s = (cudaStream_t)stream;
-  if (cudaMemsetAsync(d_nwork, 0, sizeof(uint32_t), s) != cudaSuccess) return -1;
+  if (cudaMemsetAsync(d_nwork, 0, 2 * sizeof(uint32_t), s) != cudaSuccess) return -1;
   const int blk = 256;
   uint64_t want = (count + blk - 1) / blk;
   int grid = (int)(want < (uint64_t)sm_count * 16 ? want : (uint64_t)sm_count * 16);
   mr_sieve_kernel<<<grid, blk, 0, s>>>(d_n, count, d_out, d_work, d_nwork);
-  mr_finish_kernel<<<sm_count * 8, blk, 0, s>>>(d_n, d_out, d_work, d_nwork);
+  mr_finish_kernel<<<sm_count * 8, blk, 0, s>>>(d_n, d_out, d_work, d_nwork, (uint32_t)count);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -412,7 +441,7 @@ int launch_prove_gaps(const uint64_t* d_p_after, const int32_t* d_gap, uint64_t 
 namespace voss {
 
 constexpr uint64_t kNoAllocMaxCount = 1ull << 22;  // candidates per call (16 MiB of scratch)
-constexpr uint32_t kNoAllocListOffset = 64;         // counter at [0]; list starts 256 B in
+constexpr uint32_t kNoAllocListOffset = 64;         // counters at [0], [1]; list starts 256 B in
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocMaxCount + kNoAllocListOffset];
 
@@ -462,8 +491,8 @@ extern "C" VOSS_API int voss_mr_verify_noalloc(const uint64_t* d_n, uint64_t cou
     scratch = g_noalloc_ptr[dev];
     sms = g_noalloc_sms[dev];
   }
-  // launch_mr clears the counter (cudaMemsetAsync on `scratch`) before its kernels; the list
-  // needs no clearing since entries are written before they are read.
+  // launch_mr clears the two list counters (cudaMemsetAsync on `scratch`) before its kernels;
+  // the list needs no clearing since entries are written before they are read.
   if (launch_mr(d_n, count, d_is_prime, scratch + kNoAllocListOffset, scratch, stream, sms) != 0) {
     snprintf(msg, sizeof(msg), "Miller-Rabin launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     return voss_detail::set_error(VOSS_ERR_CUDA, msg);

@@ -164,7 +164,7 @@ int sieve_kernel_attrs(int block, size_t smem, int* max_ctas_per_sm);
 void build_presieve_tables(uint32_t* out /* kPreWords */);
 int probe_smem_rmw(int sm_count, void* stream, float* ms, double* bytes);
 
-// Miller-Rabin (mr_kernels.cu).
+// Miller-Rabin (mr_kernels.cu).  d_work holds count entries, d_nwork two counters (cleared here).
 int launch_mr(const uint64_t* d_n, uint64_t count, uint8_t* d_out, uint32_t* d_work,
               uint32_t* d_nwork, void* stream, int sm_count);
 // Gap proofs: endpoints (into d_ends / d_ends_ok, 2 * count each) through the Miller-Rabin

@@ -51,6 +51,16 @@ __device__ __forceinline__ uint64_t mont_mul(uint64_t a, uint64_t b, const Mont&
   return (c1 || c2 || t2 >= M.n) ? t2 - M.n : t2;
 }
 
+// mont_mul for n < 2^63: hi + mh < 2n < 2^64 and the low-half carry keeps it <= 2n, so no
+// 64-bit overflow checks are needed.
+__device__ __forceinline__ uint64_t mont_mul_small(uint64_t a, uint64_t b, const Mont& M) {
+  const uint64_t lo = a * b;
+  const uint64_t hi = __umul64hi(a, b);
+  const uint64_t m = lo * M.ninv;
+  const uint64_t t = hi + __umul64hi(m, M.n) + (lo != 0 ? 1ull : 0ull);
+  return t >= M.n ? t - M.n : t;
+}
+
 __device__ __forceinline__ uint64_t mod_add(uint64_t a, uint64_t b, uint64_t n) {
   const uint64_t s = a + b;
   return (s < a || s >= n) ? s - n : s;
@@ -214,20 +224,43 @@ __global__ void mr_sieve_kernel(const uint64_t* __restrict__ cand, uint64_t coun
 // multiplications (the warp's longest exponent and largest r) and keeps its verdict in a flag.
 // Early exits inside these loops let the lanes of a warp drift apart and never reconverge
 // (measured: 2.8 active lanes per instruction); uniform loops keep all 32 lanes in step.
+// kSmallN: every lane's n < 2^63 (mont_mul_small).
+template <bool kSmallN = false>
 __device__ __forceinline__ bool sprp_uniform(const Mont& M, uint64_t am, uint64_t d, int r, int top_w, int r_w,
                                              bool base2) {
   uint64_t x = M.one;
   for (int b = top_w; b >= 0; --b) {
-    x = mont_mul(x, x, M);
-    const uint64_t y = base2 ? mod_add(x, x, M.n) : mont_mul(x, am, M);
+    x = kSmallN ? mont_mul_small(x, x, M) : mont_mul(x, x, M);
+    const uint64_t y = base2 ? mod_add(x, x, M.n) : (kSmallN ? mont_mul_small(x, am, M) : mont_mul(x, am, M));
     x = ((d >> b) & 1ull) ? y : x;
   }
   bool ok = (x == M.one) | (x == M.mone);
   for (int j = 0; j < r_w - 1; ++j) {
-    x = mont_mul(x, x, M);
+    x = kSmallN ? mont_mul_small(x, x, M) : mont_mul(x, x, M);
     ok |= (j < r - 1) & (x == M.mone);
   }
   return ok;
+}
+
+// Bases 3, 5, 7, ... of mr_finish_kernel for one warp: each lane stops after bases_needed(n)
+// bases or its first failure; the warp stops when no lane wants another base.
+template <bool kSmallN>
+__device__ __forceinline__ bool sprp_bases_3_on(const Mont& M, uint64_t d, int r, int top_w, int r_w, int need) {
+  const uint64_t n_ = M.n;
+  const uint64_t r1 = M.one, r2 = mod_add(r1, r1, n_), r4 = mod_add(r2, r2, n_), r6 = mod_add(r4, r2, n_);
+  uint64_t a = mod_add(r2, r1, n_);  // 3R: bases 3,5,7,11,13,17,19,23,29,31,37 by their gaps
+  bool prime = sprp_uniform<kSmallN>(M, a, d, r, top_w, r_w, false);
+#pragma unroll 1
+  for (int s = 0; s < 10; ++s) {
+    // base index s + 2 (5, 7, 11, ...): still wanted by a lane that is prime so far and needs it
+    const bool want = prime && (s + 2 < need);
+    if (!__any_sync(0xFFFFFFFFu, want)) break;
+    const int step = (0x6264242422ull >> (4 * s)) & 0xF;  // 2,2,4,2,4,2,4,6,2,6
+    a = mod_add(a, step == 2 ? r2 : (step == 4 ? r4 : r6), n_);
+    const bool pass = sprp_uniform<kSmallN>(M, a, d, r, top_w, r_w, false);
+    prime = want ? pass : prime;
+  }
+  return prime;
 }
 
 // `work` holds candidate indices (< 2^32: the entry points take fewer than 2^32 candidates per call):
@@ -254,21 +287,10 @@ __global__ void mr_finish_kernel(const uint64_t* __restrict__ cand, uint8_t* __r
     const int top = 63 - __clzll(d);
     const int top_w = __reduce_max_sync(0xFFFFFFFFu, (unsigned)top);
     const int r_w = __reduce_max_sync(0xFFFFFFFFu, (unsigned)r);
-    const uint64_t n_ = M.n;
-    const uint64_t r1 = M.one, r2 = mod_add(r1, r1, n_), r4 = mod_add(r2, r2, n_), r6 = mod_add(r4, r2, n_);
-    uint64_t a = mod_add(r2, r1, n_);  // 3R: bases 3,5,7,11,13,17,19,23,29,31,37 by their gaps
     const int need = bases_needed(n);  // >= 6: bases 2 (done) and 3 always run
-    bool prime = sprp_uniform(M, a, d, r, top_w, r_w, false);
-#pragma unroll 1
-    for (int s = 0; s < 10; ++s) {
-      // base index s + 2 (5, 7, 11, ...): still wanted by a lane that is prime so far and needs it
-      const bool want = prime && (s + 2 < need);
-      if (!__any_sync(0xFFFFFFFFu, want)) break;
-      const int step = (0x6264242422ull >> (4 * s)) & 0xF;  // 2,2,4,2,4,2,4,6,2,6
-      a = mod_add(a, step == 2 ? r2 : (step == 4 ? r4 : r6), n_);
-      const bool pass = sprp_uniform(M, a, d, r, top_w, r_w, false);
-      prime = want ? pass : prime;
-    }
+    const bool prime = __all_sync(0xFFFFFFFFu, n < (1ull << 63))
+                           ? sprp_bases_3_on<true>(M, d, r, top_w, r_w, need)
+                           : sprp_bases_3_on<false>(M, d, r, top_w, r_w, need);
     if (live) out[i] = prime ? 1 : 0;
   }
 }
@@ -352,7 +374,10 @@ __global__ void __launch_bounds__(kProveBlock) prove_interior_kernel(const uint6
             const int top = 63 - __clzll(d);
             const int top_w = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)top);
             const int r_w = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)r);
-            const bool pass = live && sprp_uniform(M, 0, d, r, top_w, r_w, true);
+            const bool small = __all_sync(0xFFFFFFFFu, v < (1ull << 63));
+            const bool prp = small ? sprp_uniform<true>(M, 0, d, r, top_w, r_w, true)
+                                   : sprp_uniform<false>(M, 0, d, r, top_w, r_w, true);
+            const bool pass = live && prp;
             if (__any_sync(0xFFFFFFFFu, pass)) {
               const bool prime = pass && sprp_rest(M, d, r);
               bad = __any_sync(0xFFFFFFFFu, prime);

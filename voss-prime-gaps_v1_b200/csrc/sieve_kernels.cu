@@ -929,22 +929,46 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
                                                             uint32_t n_iv, uint32_t* __restrict__ gbm) {
   __shared__ IntervalScatter s_iv[kScatterChunk];
   __shared__ int8_t s_rb[32];
+  __shared__ uint8_t s_wstart[240];
+  __shared__ uint8_t s_wstep[64];
   if (threadIdx.x < 32) s_rb[threadIdx.x] = c_res_bit[threadIdx.x];
+  if (threadIdx.x < 240) s_wstart[threadIdx.x] = c_walk_start[threadIdx.x];
+  if (threadIdx.x < 64) s_wstep[threadIdx.x] = c_walk_step[threadIdx.x];
   for (uint32_t i = threadIdx.x; i < n_iv; i += blockDim.x) s_iv[i] = iv[i];
   __syncthreads();
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t j = j0 + blockIdx.x * blockDim.x + threadIdx.x; j < j1; j += stride) {
     const uint32_t p = primes[j];
     const uint64_t m = magic[j];
+    const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
+    const uint8_t* row = s_wstep + bi * 8u;
     for (uint32_t s = 0; s < n_iv; ++s) {
       const IntervalScatter I = s_iv[s];
       if (p > I.sqrt_hi) break;
       const uint32_t r = mod_barrett(I.vbase, p, m);
-      uint64_t d = r ? (uint64_t)(p - r) : 0ull;
-      for (; d < I.span; d += p) {
-        const uint64_t q = d / 30ull;
-        const int b = s_rb[(uint32_t)(d - 30ull * q)];
-        if (b >= 0) atomicAnd(gbm + I.gword + (q >> 2), ~(1u << ((((uint32_t)q & 3u) << 3) | (uint32_t)b)));
+      const uint64_t d = r ? (uint64_t)(p - r) : 0ull;  // first multiple of p, offset from vbase
+      if (d >= I.span) continue;                         // none in the interval
+      const uint64_t lt = I.span / 30ull;                // bytes of the interval's bitmap
+      if (lt < (1ull << 31)) {
+        // wheel walk over the multiples p*m with gcd(m, 30) = 1 (vbase is a multiple of 30)
+        const uint32_t d32 = (uint32_t)d;
+        const uint32_t st = s_wstart[bi * 30u + (d32 - 30u * (d32 / 30u))];
+        const uint64_t off = d + (uint64_t)(st & 7u) * p;
+        if (off >= I.span) continue;
+        uint32_t byte = (uint32_t)(off / 30ull), w = st >> 3;
+        uint32_t* g = gbm + I.gword;
+        while (byte < (uint32_t)lt) {
+          const uint32_t e = row[w];
+          atomicAnd(g + (byte >> 2), ~(1u << (((byte & 3u) << 3) | (e & 7u))));
+          byte += pa * ((e >> 5) & 6u) + ((e >> 3) & 7u);
+          w = (w + 1u) & 7u;
+        }
+      } else {
+        for (uint64_t dd = d; dd < I.span; dd += p) {
+          const uint64_t q = dd / 30ull;
+          const int b = s_rb[(uint32_t)(dd - 30ull * q)];
+          if (b >= 0) atomicAnd(gbm + I.gword + (q >> 2), ~(1u << ((((uint32_t)q & 3u) << 3) | (uint32_t)b)));
+        }
       }
     }
   }

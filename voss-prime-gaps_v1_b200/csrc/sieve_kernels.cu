@@ -63,6 +63,18 @@ __device__ __forceinline__ uint32_t mod_barrett(uint64_t x, uint32_t p, uint64_t
   return (uint32_t)r;
 }
 
+// x mod p from a double-precision estimate of the quotient, for p >= 2^11 and x < 2^62:
+// xd = x and inv = 1/p rounded to double, so xd * inv is within (x/p) * 3 * 2^-53 < 2^-1 of x/p
+// and its truncation is floor(x/p) - 1, floor(x/p) or floor(x/p) + 1; one signed correction
+// finishes the remainder.
+__device__ __forceinline__ uint32_t mod_by_estimate(uint64_t x, double xd, uint32_t p, double inv) {
+  const uint64_t q = __double2ull_rz(xd * inv);
+  int64_t r = (int64_t)(x - q * (uint64_t)p);
+  if (r < 0) r += p;
+  else if (r >= (int64_t)p) r -= p;
+  return (uint32_t)r;
+}
+
 __device__ __forceinline__ uint64_t isqrt_u64(uint64_t x) {
   uint64_t s = (uint64_t)sqrt((double)x);
   if (s > 0xFFFFFFFFull) s = 0xFFFFFFFFull;
@@ -921,7 +933,7 @@ int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_int
 // them in the launch's large-prime bitmap with global atomics.  The prime table is read once
 // per launch instead of once per tile, which is what bounds high intervals (at 1e18 the table
 // is 610 MB).  The tile kernel ANDs this bitmap into its fill and skips these primes.
-constexpr int kScatterChunk = 1024;  // 32 KB of interval descriptors per block
+constexpr int kScatterChunk = 1024;  // 40 KB of interval descriptors per block
 
 __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __restrict__ primes,
                                                             const uint64_t* __restrict__ magic, uint32_t j0,
@@ -938,14 +950,14 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
   __syncthreads();
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t j = j0 + blockIdx.x * blockDim.x + threadIdx.x; j < j1; j += stride) {
-    const uint32_t p = primes[j];
-    const uint64_t m = magic[j];
+    const uint32_t p = primes[j];  // >= 8 tile spans >= 2^11 (mod_by_estimate's range)
+    const double inv = 1.0 / (double)p;
     const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
     const uint8_t* row = s_wstep + bi * 8u;
     for (uint32_t s = 0; s < n_iv; ++s) {
       const IntervalScatter I = s_iv[s];
       if (p > I.sqrt_hi) break;
-      const uint32_t r = mod_barrett(I.vbase, p, m);
+      const uint32_t r = mod_by_estimate(I.vbase, I.vbase_d, p, inv);
       const uint64_t d = r ? (uint64_t)(p - r) : 0ull;  // first multiple of p, offset from vbase
       if (d >= I.span) continue;                         // none in the interval
       const uint64_t lt = I.span / 30ull;                // bytes of the interval's bitmap

@@ -264,6 +264,7 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
       I.gword = d.gword;
       I.sqrt_hi = (uint32_t)std::min<uint64_t>(sq, 0xFFFFFFFFull);
       I.pad = 0;
+      I.vbase_d = (double)I.vbase;
       sc.push_back(I);
       wbytes += 4ull * d.n_words;
       wins.back().n++;

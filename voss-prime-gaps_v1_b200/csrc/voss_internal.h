@@ -81,6 +81,7 @@ struct IntervalScatter {
   uint64_t gword;    // first word in the large-prime bitmap
   uint32_t sqrt_hi;  // isqrt(hi - 1), capped to 2^32 - 1
   uint32_t pad;
+  double vbase_d;    // vbase rounded to double (for the quotient estimate of vbase mod p)
 };
 
 struct TilePartial {

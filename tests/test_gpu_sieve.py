@@ -162,3 +162,29 @@ def test_gaps_at_least_matches_oracle(gpu_ctx):
         np.testing.assert_array_equal(got["gap"], d[sel].astype(np.int32))
         want_m = (d[sel] / np.log(ps[sel].astype(np.float64))).astype(np.float32)
         np.testing.assert_allclose(got["merit"], want_m, rtol=4e-6)
+
+
+@pytest.mark.parametrize("compat", [True, False])
+def test_sharded_ranges_merge_to_the_whole(gpu_ctx, compat):
+    """The multi-GPU exchange of bench.py on one GPU: rank r sieves [r n + 1, (r+1) n + 1),
+    its statistics struct travels as raw bytes (the NCCL all-gather payload), and
+    voss_stats_merge adds the seam gaps; the result must equal one call over the whole range
+    (reference-compat segment boundaries fall inside and between the shards)."""
+    import voss
+    from voss import _native as N
+    world, n = 4, 10**10
+    seg = SEG if compat else 0
+    whole = gpu_ctx.sieve_range(1, world * n + 1, compat=compat, seg_num=seg, large_cap=1 << 20)
+    shards = [gpu_ctx.sieve_range(r * n + 1, (r + 1) * n + 1, compat=compat, seg_num=seg, large_cap=1 << 20)
+              for r in range(world)]
+    # counts and histograms from the raw structs alone, as bench.py gathers them
+    parts = [voss.range_result(N.RangeStats.from_buffer_copy(bytes(s.raw))) for s in shards]
+    m = voss.merge_stats(parts)
+    for k in ("prime_count", "first_prime", "last_prime", "max_gap", "max_gap_lo", "large_total"):
+        assert getattr(m, k) == getattr(whole, k), k
+    for k in ("mod4", "modq", "modq_gap", "gap_hist"):
+        np.testing.assert_array_equal(getattr(m, k), getattr(whole, k), err_msg=k)
+    # with the large-gap lists as well
+    m2 = voss.merge_stats(shards)
+    assert sorted(zip(m2.large["position"].tolist(), m2.large["gap"].tolist())) == \
+        sorted(zip(whole.large["position"].tolist(), whole.large["gap"].tolist()))

@@ -496,6 +496,38 @@ int run_range_device(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t flags, uint
   return VOSS_OK;
 }
 
+// The first n device large-gap records, sorted by position on the device (positions < hi), in
+// the context's pinned staging.
+int stage_large_sorted(voss_ctx* c, uint64_t n, uint64_t hi, voss_large_gap** out) {
+  if (n > c->h_large_cap) {
+    if (c->h_large) cudaFreeHost(c->h_large);
+    c->h_large = nullptr;
+    c->h_large_cap = 0;
+    const size_t cap = (size_t)n + n / 4 + 1024;
+    if (cudaMallocHost(&c->h_large, cap * sizeof(voss_large_gap)) != cudaSuccess) {
+      c->h_large = nullptr;
+      return fail(VOSS_ERR_NOMEM, "cudaMallocHost of the large-gap staging failed");
+    }
+    c->h_large_cap = cap;
+  }
+  *out = c->h_large;
+  if (n == 0) return VOSS_OK;
+  Workspace& W = c->ws;
+  cudaStream_t s = c->stream;
+  const int end_bit = hi > 1 ? 64 - __builtin_clzll(hi - 1) : 1;  // bits in which positions can differ
+  const size_t tb = large_sort_temp_bytes((uint32_t)n, end_bit);
+  int rc;
+  if ((rc = W.ls_keys.ensure(16 * n)) || (rc = W.ls_idx.ensure(8 * n)) || (rc = W.ls_temp.ensure(std::max<size_t>(tb, 1))) ||
+      (rc = W.ls_sorted.ensure(sizeof(voss_large_gap) * n)))
+    return rc;
+  if (launch_large_sort(W.large.as<LargeGapDev>(), (uint32_t)n, end_bit, W.ls_keys.as<unsigned long long>(),
+                        W.ls_idx.as<uint32_t>(), W.ls_temp.p, tb, W.ls_sorted.as<LargeGapDev>(), c->sm_count, s))
+    return fail(VOSS_ERR_CUDA, "large-gap sort failed: %s", cudaGetErrorString(cudaGetLastError()));
+  CUDA_TRY(cudaMemcpyAsync(c->h_large, W.ls_sorted.p, sizeof(voss_large_gap) * n, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return VOSS_OK;
+}
+
 int fetch_range(voss_ctx* c, voss_range_stats* st, voss_large_gap* large, uint64_t large_cap,
                 uint64_t* written) {
   if (!c->have_range) return fail(VOSS_ERR_STATE, "no range has been sieved on this context");
@@ -511,14 +543,12 @@ int fetch_range(voss_ctx* c, voss_range_stats* st, voss_large_gap* large, uint64
   const uint64_t found = ctr[kCtrLarge];
   st->large_total = found;
   const uint64_t ondev = std::min<uint64_t>(found, c->r_large_cap);
-  std::vector<voss_large_gap> lg(ondev);
-  if (ondev)
-    CUDA_TRY(cudaMemcpy(lg.data(), c->ws.large.p, sizeof(voss_large_gap) * ondev, cudaMemcpyDeviceToHost));
-  std::sort(lg.begin(), lg.end(), [](const voss_large_gap& x, const voss_large_gap& y) {
-    return x.position < y.position;
-  });
   const uint64_t w = std::min<uint64_t>(ondev, large ? large_cap : 0);
-  if (w) std::memcpy(large, lg.data(), sizeof(voss_large_gap) * w);
+  if (w) {
+    voss_large_gap* lg = nullptr;
+    if ((rc = stage_large_sorted(c, ondev, c->r_hi, &lg))) return rc;
+    std::memcpy(large, lg, sizeof(voss_large_gap) * w);
+  }
   if (written) *written = w;
   return VOSS_OK;
 }
@@ -598,6 +628,7 @@ VOSS_API void voss_ctx_destroy(voss_ctx* c) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->h_large) cudaFreeHost(c->h_large);
   delete c;
 }
 
@@ -723,10 +754,9 @@ VOSS_API int voss_gaps_at_least(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t 
   *count = found;
   const uint64_t w = std::min<uint64_t>(std::min<uint64_t>(found, devcap), cap);
   if (w) {
-    std::vector<voss_large_gap> v(std::min<uint64_t>(found, devcap));
-    CUDA_TRY(cudaMemcpy(v.data(), c->ws.large.p, sizeof(voss_large_gap) * v.size(), cudaMemcpyDeviceToHost));
-    std::sort(v.begin(), v.end(), [](const voss_large_gap& x, const voss_large_gap& y) { return x.position < y.position; });
-    std::memcpy(out, v.data(), sizeof(voss_large_gap) * w);
+    voss_large_gap* v = nullptr;
+    if ((rc = stage_large_sorted(c, std::min<uint64_t>(found, devcap), hi, &v))) return rc;
+    std::memcpy(out, v, sizeof(voss_large_gap) * w);
   }
   return VOSS_OK;
 }

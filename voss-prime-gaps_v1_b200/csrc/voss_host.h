@@ -45,6 +45,7 @@ struct Workspace {
   DevBuf gbm, scat;  // large-prime pre-pass: bitmap of the launch and its interval descriptors
   DevBuf pg_pa, pg_gap, pg_ok;  // gap proofs: inputs and verdicts (endpoints use mr_in / mr_out / mr_work)
   DevBuf sha_data, sha_off, sha_out;  // certificate hashing: messages, offsets, digests
+  DevBuf ls_keys, ls_idx, ls_temp, ls_sorted;  // large-gap list sorted by position (large_sort.cu)
   // Largest large-prime bitmap this workspace may use; with gbm_fixed the buffers are never
   // grown (server slots size them at creation), and launches that need more skip the pre-pass.
   size_t gbm_budget = 8ull << 30;
@@ -93,6 +94,10 @@ struct voss_ctx {
   uint32_t r_tiles = 0;
   uint64_t r_large_cap = 0;
   float sieve_ms = 0, total_ms = 0;
+  // host side of the large-gap list: pinned, grow-only staging for the device-to-host copy of
+  // the list (sorted on the device), so that repeated calls touch no fresh pages
+  voss_large_gap* h_large = nullptr;
+  size_t h_large_cap = 0;
 };
 
 namespace voss_host {

@@ -162,6 +162,10 @@ int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_int
 int launch_scatter_large(const uint32_t* primes, const uint64_t* magic, uint32_t j0, uint32_t j1,
                          const IntervalScatter* iv, uint32_t n_iv, uint32_t* gbm, int sm_count, void* stream);
 int sieve_kernel_attrs(int block, size_t smem, int* max_ctas_per_sm);
+// Large-gap list sorted by position on the device (large_sort.cu): keys and idx hold 2n entries.
+size_t large_sort_temp_bytes(uint32_t n, int end_bit);
+int launch_large_sort(const LargeGapDev* in, uint32_t n, int end_bit, unsigned long long* keys, uint32_t* idx,
+                      void* temp, size_t temp_bytes, LargeGapDev* out, int sm_count, void* stream);
 void build_presieve_tables(uint32_t* out /* kPreWords */);
 int probe_smem_rmw(int sm_count, void* stream, float* ms, double* bytes);
 

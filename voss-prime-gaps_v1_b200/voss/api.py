@@ -121,11 +121,20 @@ class Context:
         N.check(self.lib.voss_ctx_set_tuning(self._h, byref(t)))
         return self.tuning()
 
+    def _large_buffer(self, cap: int) -> np.ndarray:
+        """A reused output buffer for large-gap lists (only the written part is copied out), so
+        that repeated calls touch no fresh pages."""
+        buf = getattr(self, "_large_buf", None)
+        if buf is None or buf.size < cap:
+            buf = np.empty(max(cap, 1), dtype=LARGE_DTYPE)
+            self._large_buf = buf
+        return buf[:max(cap, 1)]
+
     # -- sieve ------------------------------------------------------------------------------
     def sieve_range(self, lo: int, hi: int, compat: bool = False, seg_num: int = 30_000_000_000,
                     large_cap: int = 1 << 22) -> RangeResult:
         st = N.RangeStats()
-        large = np.zeros(large_cap, dtype=LARGE_DTYPE)
+        large = self._large_buffer(large_cap)
         w = c_uint64()
         N.check(self.lib.voss_sieve_range(
             self._h, lo, hi, N.FLAG_REF_COMPAT if compat else 0, seg_num if compat else 0, byref(st),
@@ -139,7 +148,7 @@ class Context:
 
     def fetch_range(self, large_cap: int = 1 << 22) -> RangeResult:
         st = N.RangeStats()
-        large = np.zeros(large_cap, dtype=LARGE_DTYPE)
+        large = self._large_buffer(large_cap)
         w = c_uint64()
         N.check(self.lib.voss_fetch_range(self._h, byref(st), large.ctypes.data_as(ctypes.POINTER(N.LargeGap)),
                                           large_cap, byref(w)))
@@ -165,11 +174,11 @@ class Context:
         if cap is None:
             cap = 1 << 20
         while True:
-            out = np.zeros(max(cap, 1), dtype=LARGE_DTYPE)
+            out = np.empty(max(cap, 1), dtype=LARGE_DTYPE)
             N.check(self.lib.voss_gaps_at_least(self._h, lo, hi, min_gap,
                                                 out.ctypes.data_as(ctypes.POINTER(N.LargeGap)), cap, byref(cnt)))
             if cnt.value <= cap:
-                return out[: cnt.value]
+                return out[: cnt.value].copy()
             cap = cnt.value
 
     def sieve_intervals(self, lo, hi) -> np.ndarray:
@@ -196,7 +205,7 @@ class Context:
         """voss_run_checkpointed: [1, n] segment by segment with checkpoint.bin / stop.txt in
         `directory`.  Returns (RangeResult, resumed_from); raises VossError(-7) when stopped."""
         st = N.RangeStats()
-        large = np.zeros(large_cap, dtype=LARGE_DTYPE)
+        large = np.empty(large_cap, dtype=LARGE_DTYPE)  # only the written part is kept
         w, res = c_uint64(), c_uint64()
         N.check(self.lib.voss_run_checkpointed(self._h, n, seg_num, N.FLAG_REF_COMPAT if compat else 0, ckpt_every,
                                                directory.encode(), byref(st),
@@ -311,7 +320,7 @@ def run_checkpointed_fn(segment, n: int, seg_num: int, compat: bool, ckpt_every:
 
     fn = N.SEGMENT_FN(cb)
     st = N.RangeStats()
-    large = np.zeros(large_cap, dtype=LARGE_DTYPE)
+    large = np.empty(large_cap, dtype=LARGE_DTYPE)  # only the written part is kept
     w, res = c_uint64(), c_uint64()
     N.check(lib.voss_run_checkpointed_fn(fn, None, n, seg_num, N.FLAG_REF_COMPAT if compat else 0, ckpt_every,
                                          directory.encode(), byref(st),

@@ -594,6 +594,8 @@ VOSS_API int voss_ctx_create(int device, uint64_t max_hi, voss_ctx** out) {
   if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return bail(fail(VOSS_ERR_CUDA, "cudaGetDeviceProperties failed"));
   c->sm_count = prop.multiProcessorCount;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_copy, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaEventCreate(&c->ev2) != cudaSuccess)
     return bail(fail(VOSS_ERR_CUDA, "stream/event creation failed"));
@@ -628,6 +630,8 @@ VOSS_API void voss_ctx_destroy(voss_ctx* c) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->ev_copy) cudaEventDestroy(c->ev_copy);
   if (c->h_large) cudaFreeHost(c->h_large);
   delete c;
 }
@@ -830,12 +834,29 @@ VOSS_API int voss_mr_verify(voss_ctx* c, const uint64_t* n, uint64_t count, uint
   if (count > 0xFFFFFFFFull) return fail(VOSS_ERR_ARG, "count must be < 2^32 per call");
   cudaSetDevice(c->device);
   cudaStream_t s = c->stream;
+  Workspace& W = c->ws;
   int rc;
-  // context-owned, grow-only buffers: repeated calls do not allocate
-  if ((rc = c->ws.mr_in.ensure(count * 8)) || (rc = c->ws.mr_out.ensure(count))) return rc;
-  CUDA_TRY(cudaMemcpyAsync(c->ws.mr_in.p, n, count * 8, cudaMemcpyHostToDevice, s));
-  if ((rc = voss_mr_verify_device(c, c->ws.mr_in.as<uint64_t>(), count, c->ws.mr_out.as<uint8_t>(), s))) return rc;
-  CUDA_TRY(cudaMemcpyAsync(is_prime, c->ws.mr_out.p, count, cudaMemcpyDeviceToHost, s));
+  // context-owned, grow-only buffers: repeated calls do not allocate.  The candidates cross in
+  // chunks on the copy stream while the previous chunk is tested on `stream` (a copy from
+  // pageable memory returns once staged, without waiting for the device); the verdicts come
+  // back in one copy at the end (a device-to-host copy into pageable memory would block).
+  constexpr uint64_t kChunk = 1ull << 24;
+  const uint64_t per = std::min(count, kChunk);
+  if ((rc = W.mr_in.ensure(count * 8)) || (rc = W.mr_out.ensure(count)) ||
+      (rc = W.mr_work.ensure(sizeof(uint32_t) * (per + 8))))
+    return rc;
+  uint64_t* d_in = W.mr_in.as<uint64_t>();
+  uint8_t* d_out = W.mr_out.as<uint8_t>();
+  uint32_t* work = W.mr_work.as<uint32_t>();
+  for (uint64_t off = 0; off < count; off += kChunk) {
+    const uint64_t k = std::min(kChunk, count - off);
+    CUDA_TRY(cudaMemcpyAsync(d_in + off, n + off, k * 8, cudaMemcpyHostToDevice, c->copy_stream));
+    CUDA_TRY(cudaEventRecord(c->ev_copy, c->copy_stream));
+    CUDA_TRY(cudaStreamWaitEvent(s, c->ev_copy, 0));
+    if (launch_mr(d_in + off, k, d_out + off, work + 8, work, s, c->sm_count))
+      return fail(VOSS_ERR_CUDA, "Miller-Rabin launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  CUDA_TRY(cudaMemcpyAsync(is_prime, d_out, count, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   return VOSS_OK;
 }

@@ -80,6 +80,8 @@ struct voss_ctx {
   int device = 0;
   int sm_count = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // host-to-device copies overlapped with work on `stream`
+  cudaEvent_t ev_copy = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   uint64_t max_hi = 0;
   std::vector<uint32_t> primes;  // >= 37

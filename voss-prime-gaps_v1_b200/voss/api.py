@@ -186,7 +186,7 @@ class Context:
         hi = np.ascontiguousarray(hi, dtype=np.uint64)
         if lo.shape != hi.shape:
             raise ValueError("lo and hi differ in shape")
-        out = np.zeros(lo.size, dtype=INTERVAL_DTYPE)
+        out = np.empty(lo.size, dtype=INTERVAL_DTYPE)  # every record is written by the call
         N.check(self.lib.voss_sieve_intervals(self._h, _u64p(lo), _u64p(hi), lo.size,
                                               out.ctypes.data_as(ctypes.POINTER(N.IntervalStats))))
         return out

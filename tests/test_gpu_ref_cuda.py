@@ -20,7 +20,7 @@ EXACT = ["gap_histogram.csv", "hl_trend.csv", "modq_counts.csv", "modq_gap_hist.
          "gap_sequence.csv"]
 
 
-@pytest.mark.parametrize("n", [10**9, 10**10, 10**11])
+@pytest.mark.parametrize("n", [10**9, 10**10, 10**11, 10**12])
 def test_artifacts_equal_reference_program(gpu_ctx, n):
     import voss
     exe = os.path.join(O.REF_BIN_DIR, f"voss_v7_live_{n}")

@@ -144,6 +144,7 @@ extern "C" {
 
 VOSS_API int voss_sha256_batch(voss_ctx* c, const uint8_t* data, const uint64_t* offsets, uint64_t count,
                                uint8_t* digests) {
+  NvtxRange nvtx_("voss_sha256_batch");
   if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
   if (count == 0) return VOSS_OK;
   if (!offsets || !digests) return fail(VOSS_ERR_ARG, "NULL argument");

@@ -450,6 +450,7 @@ void finalize_range(const unsigned long long* acc, const IntervalOut& o, uint64_
 int fetch_common(voss_ctx* c, uint32_t n_iv, std::vector<unsigned long long>& acc,
                  std::vector<IntervalOut>& outs, uint32_t* ctr, std::vector<OverflowGap>& over,
                  bool want_acc) {
+  NvtxRange r("fetch statistics");
   cudaStream_t s = c->stream;
   CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(uint32_t) * kCtrWords, cudaMemcpyDeviceToHost, s));
   outs.resize(std::max<uint32_t>(1, n_iv));
@@ -482,9 +483,16 @@ int run_range_device(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t flags, uint
       return fail(VOSS_ERR_ARG, "seg_num/30 = %" PRIu64 " is below the tile size %" PRIu64 " bytes", seg_k, tile_bytes);
   }
   RunPlan P;
-  int rc = plan_intervals(c, &lo, &hi, 1, seg_k, &P);
+  int rc;
+  {
+    NvtxRange r("plan");
+    rc = plan_intervals(c, &lo, &hi, 1, seg_k, &P);
+  }
   if (rc) return rc;
-  rc = launch_plan(c, P, true, large_cap, false, s);
+  {
+    NvtxRange r("launch");
+    rc = launch_plan(c, P, true, large_cap, false, s);
+  }
   if (rc) return rc;
   c->have_range = true;
   c->r_lo = lo;
@@ -512,6 +520,7 @@ int stage_large_sorted(voss_ctx* c, uint64_t n, uint64_t hi, voss_large_gap** ou
   }
   *out = c->h_large;
   if (n == 0) return VOSS_OK;
+  NvtxRange r("sort and copy large gaps");
   Workspace& W = c->ws;
   cudaStream_t s = c->stream;
   const int end_bit = hi > 1 ? 64 - __builtin_clzll(hi - 1) : 1;  // bits in which positions can differ
@@ -539,7 +548,10 @@ int fetch_range(voss_ctx* c, voss_range_stats* st, voss_large_gap* large, uint64
   if (rc) return rc;
   cudaEventElapsedTime(&c->sieve_ms, c->ev0, c->ev1);
   cudaEventElapsedTime(&c->total_ms, c->ev0, c->ev2);
-  finalize_range(acc.data(), outs[0], c->r_lo, c->r_hi, c->r_flags, c->r_seg, over, st);
+  {
+    NvtxRange r("finalize statistics");
+    finalize_range(acc.data(), outs[0], c->r_lo, c->r_hi, c->r_flags, c->r_seg, over, st);
+  }
   const uint64_t found = ctr[kCtrLarge];
   st->large_total = found;
   const uint64_t ondev = std::min<uint64_t>(found, c->r_large_cap);
@@ -664,6 +676,7 @@ VOSS_API int voss_ctx_get_tuning(const voss_ctx* c, voss_tuning* t) {
 
 VOSS_API int voss_sieve_range_device(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t flags,
                                      uint64_t seg_num, void* stream) {
+  NvtxRange nvtx_("voss_sieve_range_device");
   if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
   cudaSetDevice(c->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
@@ -681,6 +694,7 @@ VOSS_API int voss_sieve_range_device(voss_ctx* c, uint64_t lo, uint64_t hi, uint
 
 VOSS_API int voss_fetch_range(voss_ctx* c, voss_range_stats* st, voss_large_gap* large,
                               uint64_t large_cap, uint64_t* written) {
+  NvtxRange nvtx_("voss_fetch_range");
   if (!c || !st) return fail(VOSS_ERR_ARG, "NULL argument");
   cudaSetDevice(c->device);
   return fetch_range(c, st, large, large_cap, written);
@@ -689,6 +703,7 @@ VOSS_API int voss_fetch_range(voss_ctx* c, voss_range_stats* st, voss_large_gap*
 VOSS_API int voss_sieve_range(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t flags, uint64_t seg_num,
                               voss_range_stats* st, voss_large_gap* large, uint64_t large_cap,
                               uint64_t* written) {
+  NvtxRange nvtx_("voss_sieve_range");
   if (!c || !st) return fail(VOSS_ERR_ARG, "NULL argument");
   cudaSetDevice(c->device);
   int rc = run_range_device(c, lo, hi, flags, seg_num, std::max(large_cap, kDefaultLargeCap), c->stream);
@@ -710,6 +725,7 @@ VOSS_API int voss_last_kernel_ms(const voss_ctx* c, double* sieve_ms, double* to
 
 VOSS_API int voss_sieve_intervals(voss_ctx* c, const uint64_t* lo, const uint64_t* hi, uint32_t n,
                                   voss_interval_stats* out) {
+  NvtxRange nvtx_("voss_sieve_intervals");
   if (!c || (n && (!lo || !hi || !out))) return fail(VOSS_ERR_ARG, "NULL argument");
   cudaSetDevice(c->device);
   for (uint32_t i = 0; i < n; ++i) {
@@ -739,6 +755,7 @@ VOSS_API int voss_sieve_intervals(voss_ctx* c, const uint64_t* lo, const uint64_
 
 VOSS_API int voss_gaps_at_least(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t min_gap, voss_large_gap* out,
                                 uint64_t cap, uint64_t* count) {
+  NvtxRange nvtx_("voss_gaps_at_least");
   if (!c || !count || (cap && !out)) return fail(VOSS_ERR_ARG, "NULL argument");
   if (min_gap < 3) return fail(VOSS_ERR_ARG, "min_gap must be at least 3");
   if (hi < lo) return fail(VOSS_ERR_ARG, "hi < lo");
@@ -767,6 +784,7 @@ VOSS_API int voss_gaps_at_least(voss_ctx* c, uint64_t lo, uint64_t hi, uint32_t 
 
 VOSS_API int voss_primes_range(voss_ctx* c, uint64_t lo, uint64_t hi, uint64_t* out, uint64_t cap,
                                uint64_t* count) {
+  NvtxRange nvtx_("voss_primes_range");
   if (!c || !count || (cap && !out)) return fail(VOSS_ERR_ARG, "NULL argument");
   if (hi < lo) return fail(VOSS_ERR_ARG, "hi < lo");
   if (hi > c->max_hi) return fail(VOSS_ERR_RANGE, "hi exceeds the context limit");
@@ -814,6 +832,7 @@ VOSS_API int voss_primes_range(voss_ctx* c, uint64_t lo, uint64_t hi, uint64_t* 
 
 VOSS_API int voss_mr_verify_device(voss_ctx* c, const uint64_t* d_n, uint64_t count, uint8_t* d_out,
                                    void* stream) {
+  NvtxRange nvtx_("voss_mr_verify_device");
   if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
   if (count && (!d_n || !d_out)) return fail(VOSS_ERR_ARG, "NULL argument");
   if (count > 0xFFFFFFFFull) return fail(VOSS_ERR_ARG, "count must be < 2^32 per call");
@@ -828,6 +847,7 @@ VOSS_API int voss_mr_verify_device(voss_ctx* c, const uint64_t* d_n, uint64_t co
 }
 
 VOSS_API int voss_mr_verify(voss_ctx* c, const uint64_t* n, uint64_t count, uint8_t* is_prime) {
+  NvtxRange nvtx_("voss_mr_verify");
   if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
   if (count == 0) return VOSS_OK;
   if (!n || !is_prime) return fail(VOSS_ERR_ARG, "NULL argument");
@@ -863,6 +883,7 @@ VOSS_API int voss_mr_verify(voss_ctx* c, const uint64_t* n, uint64_t count, uint
 
 VOSS_API int voss_prove_gaps(voss_ctx* c, const uint64_t* p_after, const int32_t* gap, uint64_t count,
                              uint8_t* ok) {
+  NvtxRange nvtx_("voss_prove_gaps");
   if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
   if (count == 0) return VOSS_OK;
   if (!p_after || !gap || !ok) return fail(VOSS_ERR_ARG, "NULL argument");

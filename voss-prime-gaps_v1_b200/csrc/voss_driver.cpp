@@ -96,6 +96,7 @@ const char kMagic[8] = {'V', 'O', 'S', 'S', 'C', 'K', 'P', '1'};
 
 int save_ckpt(const std::string& path, const CkptHeader& h, const voss_range_stats& st,
               const std::vector<voss_large_gap>& large) {
+  NvtxRange nvtx_("checkpoint write");
   const std::string tmp = path + ".tmp";
   FILE* f = std::fopen(tmp.c_str(), "wb");
   if (!f) return fail(VOSS_ERR_IO, "cannot write %s", tmp.c_str());
@@ -139,6 +140,7 @@ extern "C" {
 
 VOSS_API int voss_gap_sequence(voss_ctx* c, uint64_t n, uint64_t seg_num, uint64_t seq_size, int32_t* gap,
                                uint64_t* p_lo, uint64_t* written) {
+  NvtxRange nvtx_("voss_gap_sequence");
   if (!c || (seq_size && (!gap || !p_lo))) return fail(VOSS_ERR_ARG, "NULL argument");
   if (seg_num == 0 || seg_num % 30) return fail(VOSS_ERR_ARG, "seg_num must be a positive multiple of 30");
   if (n + 1 > c->max_hi) return fail(VOSS_ERR_RANGE, "n exceeds the context limit");
@@ -196,6 +198,7 @@ VOSS_API int voss_run_checkpointed_fn(voss_segment_fn fn, void* user, uint64_t n
                                       uint32_t ckpt_every, const char* dir, voss_range_stats* out,
                                       voss_large_gap* large, uint64_t large_cap, uint64_t* large_written,
                                       uint64_t* resumed_from) {
+  NvtxRange nvtx_("voss_run_checkpointed_fn");
   if (!fn || !dir || !out) return fail(VOSS_ERR_ARG, "NULL argument");
   if (n < 1 || seg_num == 0 || seg_num % 30) return fail(VOSS_ERR_ARG, "need n >= 1 and seg_num a positive multiple of 30");
   if (!ckpt_every) ckpt_every = 5;

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <vector>
@@ -14,6 +15,27 @@ namespace voss_host {
 
 // Record a message for voss_last_error() and return `code`.
 int fail(int code, const char* fmt, ...);
+
+// NVTX range in the "voss" domain for the lifetime of the object: every API call and its host
+// stages (plan, launch, sort, copy) show as named spans on an Nsight Systems timeline.  NVTX 3
+// is header-only; with no tool attached a push/pop is a test of one pointer.
+inline nvtxDomainHandle_t nvtx_domain() {
+  static nvtxDomainHandle_t d = nvtxDomainCreateA("voss");
+  return d;
+}
+struct NvtxRange {
+  explicit NvtxRange(const char* name) {
+    nvtxEventAttributes_t a = {};
+    a.version = NVTX_VERSION;
+    a.size = NVTX_EVENT_ATTRIB_STRUCT_SIZE;
+    a.messageType = NVTX_MESSAGE_TYPE_ASCII;
+    a.message.ascii = name;
+    nvtxDomainRangePushEx(nvtx_domain(), &a);
+  }
+  ~NvtxRange() { nvtxDomainRangePop(nvtx_domain()); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 #define CUDA_TRY(call)                                                                      \
   do {                                                                                      \

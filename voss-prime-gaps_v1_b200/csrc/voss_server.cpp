@@ -110,6 +110,7 @@ void CUDART_CB on_slot_done(void* p) {
 // Queue one batch on a free slot (called without the server lock; the batch lists are owned by
 // the scheduler thread until completion).
 int launch_batch(voss_server* S, Slot& sl) {
+  NvtxRange nvtx_("server batch launch");
   voss_ctx* c = S->ctx;
   cudaStream_t s = sl.stream;
   sl.n_iv = (uint32_t)sl.iv.size();
@@ -156,6 +157,7 @@ int launch_batch(voss_server* S, Slot& sl) {
 
 // Deliver a finished slot's results (called with the server lock held).
 void complete_slot(voss_server* S, Slot& sl) {
+  NvtxRange nvtx_("server batch complete");
   const auto now = Clock::now();
   int err = sl.launch_error;
   if (!err && sl.n_iv) err = check_device_error(sl.h_ctr);

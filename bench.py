@@ -173,6 +173,96 @@ def sieve_work(n: int) -> int:
     return int((upto(n // p) - upto(p - 1)).sum())
 
 
+def primes_upto(s: int):
+    """Primes 7 <= p <= s as float64 (numpy sieve of Eratosthenes)."""
+    import numpy as np
+    flags = np.ones(s + 1, dtype=bool)
+    flags[:2] = False
+    for q in range(2, math.isqrt(s) + 1):
+        if flags[q]:
+            flags[q * q::q] = False
+    p = np.nonzero(flags)[0]
+    return p[p >= 7].astype(np.float64)
+
+
+def interval_work(lo, hi, p_large: int) -> dict:
+    """Algorithmic work terms of a batch of intervals [lo_i, hi_i).
+
+    offsets: one first-hit computation per (interval, base prime 7 <= p <= isqrt(hi_i - 1)).
+    Bit-clears: for each such prime, the multiples of p in [max(lo_i, p^2), hi_i) coprime to 30,
+    taken as their expected count 8 (hi_i - max(lo_i, p^2)) / (30 p); split into the primes
+    7..31 (applied as word masks, no clears), 37 <= p < p_large (cleared in shared memory by the
+    tile kernel) and p >= p_large (the large-prime pre-pass).  Expected rather than exact counts:
+    exact ones would take one division per (interval, prime), ~10^10 on the host here."""
+    import numpy as np
+    P = primes_upto(math.isqrt(int(hi.max()) - 1))
+    inv = np.concatenate([[0.0], np.cumsum(1.0 / P)])
+    cuts = [7.0, 37.0, float(p_large), math.inf]  # presieve | tile | pre-pass
+    offsets = 0
+    hits = [0.0, 0.0, 0.0]
+    for a, b in zip(lo.tolist(), hi.tolist()):
+        if b <= a:
+            continue
+        s_hi = math.isqrt(b - 1)
+        s_lo = math.isqrt(a)  # p <= s_lo: p^2 <= lo, multiples from lo
+        n_hi = int(np.searchsorted(P, s_hi, side="right"))
+        n_lo = min(int(np.searchsorted(P, s_lo, side="right")), n_hi)
+        offsets += n_hi
+        big = P[n_lo:n_hi]  # lo < p^2 < hi: multiples from p^2
+        for c in range(3):
+            i0 = int(np.searchsorted(P, cuts[c], side="left"))
+            i1 = int(np.searchsorted(P, cuts[c + 1], side="left")) if cuts[c + 1] != math.inf else P.size
+            j1 = min(i1, n_lo)
+            if j1 > i0:
+                hits[c] += (b - a) * (inv[j1] - inv[i0])
+            sel = big[(big >= cuts[c]) & (big < cuts[c + 1])]
+            if sel.size:
+                hits[c] += float(((b - sel * sel) / sel).sum())
+    k = 8.0 / 30.0
+    return {"first_hit_offsets": int(offsets), "presieve_primes_hits": k * hits[0],
+            "tile_hits": k * hits[1], "prepass_hits": k * hits[2], "p_large": int(p_large),
+            "note": "hits are expected counts, 8(hi - max(lo, p^2))/(30p) per (interval, prime)"}
+
+
+_MR_BASES = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37)
+
+
+def mr_mulmods(sample) -> tuple[int, int]:
+    """Montgomery products the Miller-Rabin kernels' algorithm needs for these candidates,
+    (moduli below 2^63, moduli above): per candidate that trial division by 2..37 leaves open,
+    for each base in order up to the first that fails, or up to as many bases as n's size needs
+    (6, 7, 9 or 12): one squaring per bit of the odd part d, one product per set bit of d (none
+    for base 2, whose products are doublings), and the squarings of the r - 1 follow-up steps
+    up to the first -1.  The lanes' padding in the warp-uniform loops is overhead, not counted."""
+    small = full = 0
+    for n in map(int, sample):
+        if n < 2 or n % 2 == 0 or any(n == b or n % b == 0 for b in _MR_BASES[1:]):
+            continue
+        d = n - 1
+        r = (d & -d).bit_length() - 1
+        d >>= r
+        bits, ones = d.bit_length(), bin(d).count("1")
+        need = 6 if n < 3474749660383 else 7 if n < 341550071728321 else 9 if n < 3825123056546413051 else 12
+        cnt = 0
+        for a in _MR_BASES[:need]:
+            cnt += bits + (0 if a == 2 else ones)
+            x = pow(a, d, n)
+            ok = x == 1 or x == n - 1
+            j = 0
+            while not ok and j < r - 1:
+                x = x * x % n
+                j += 1
+                cnt += 1
+                ok = x == n - 1
+            if not ok:
+                break
+        if n < 1 << 63:
+            small += cnt
+        else:
+            full += cnt
+    return small, full
+
+
 # ---------------------------------------------------------------------------------------
 def cpu_baseline(n: int, seconds: float, ranges_done=None) -> dict:
     """Oracle OpenMP interval sieve (port of verify_cpp's marking loop) on the top of [1, n]."""
@@ -276,7 +366,10 @@ def run_intervals(a) -> None:
         ctx.sieve_intervals(lo, hi)
     # the base-prime table (69 MB) fits in L2: flush it between timed steps
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda:0")
-    dev_ms, wall = [], []
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    dev_ms, wall, phases = [], [], []
     for _ in range(a.steps):
         flush.add_(1)
         torch.cuda.synchronize()
@@ -284,6 +377,8 @@ def run_intervals(a) -> None:
         batched = ctx.sieve_intervals(lo, hi)
         wall.append(time.perf_counter() - t0)
         dev_ms.append(ctx.last_kernel_ms()[1])
+        phases.append(ctx.last_phase_ms())
+    clk = clocks.stop()
     # one plain launch per interval
     plain_wall = 0.0
     plain_dev = 0.0
@@ -298,6 +393,14 @@ def run_intervals(a) -> None:
     total_int = float((hi - lo).sum())
     bw = statistics.mean(wall)
     bd = statistics.mean(dev_ms) * 1e-3
+    pre_ms, tile_ms, tail_ms = (statistics.mean(ph[k] for ph in phases) for k in range(3))
+    t = ctx.tuning()
+    tile_bytes = 4 * t["block_threads"] * t["chunk_words"]
+    work = interval_work(lo, hi, t["mult_factor"] * tile_bytes)
+    smem_peak = ctx.probe_smem_rmw()
+    # tile kernel: 8 B per shared-memory bit-clear + one read of the intervals' bitmap words
+    alg_bytes = 8.0 * work["tile_hits"] + total_int / 30.0
+    achieved = alg_bytes / (tile_ms * 1e-3) / 1e9
     out = {
         "metric": "mixed-interval queries/s (4096 seeded intervals, batched persistent launch)",
         "value": lo.size / bd, "unit": "intervals/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
@@ -309,6 +412,16 @@ def run_intervals(a) -> None:
         "integers_per_s": total_int / bd,
         "e2e": {"value": lo.size / bw, "unit": "intervals/s", "h2d_bytes_per_step": 48 * int(lo.size),
                 "d2h_bytes_per_step": batched.itemsize * int(lo.size) + 32},
+        "phases_ms": {"copies_memsets_prepass": pre_ms, "tile_kernel": tile_ms, "stitch_reduce_finalize": tail_ms},
+        "work_terms": work,
+        "prepass_clears_per_s": work["prepass_hits"] / (pre_ms * 1e-3) if pre_ms > 0 else None,
+        "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
+                     "frac": achieved / smem_peak, "traffic": None, "kernel": "sieve_tiles_kernel",
+                     "kernel_ms": tile_ms, "algorithmic_bytes": alg_bytes,
+                     "peak_source": "voss_probe_smem_rmw (this GPU, this run)",
+                     "traffic_note": "DRAM traffic of this launch: profiles/launches_intervals_4096.md"},
+        "clocks": clk,
+        "gpu_launches": a.steps * phases[-1][3],
     }
     if not a.no_plain:
         out["plain_launch_per_interval"] = {"value": lo.size / plain_dev * 1e3, "unit": "intervals/s (device)",
@@ -349,13 +462,26 @@ def run_mr(a) -> None:
     for _ in range(a.warmup):
         ctx.mr_verify_device(d_n.data_ptr(), n.size, d_out.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
     for e0, e1 in ev:
         e0.record(stream)
         ctx.mr_verify_device(d_n.data_ptr(), n.size, d_out.data_ptr(), stream.cuda_stream)
         e1.record(stream)
     torch.cuda.synchronize()
+    clk = clocks.stop()
     ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+    # roofline: Montgomery products the algorithm needs (counted on a seeded sample of the
+    # batch, scaled) against this GPU's measured product rate, per modulus class
+    msample = n[: min(n.size, 100_000)]
+    m_small, m_full = mr_mulmods(msample)
+    scale = n.size / msample.size
+    m_small, m_full = m_small * scale, m_full * scale
+    peak_full, peak_small = ctx.probe_mulmod()
+    t_ideal = m_small / peak_small + m_full / peak_full
+    t_meas = ms * 1e-3
     got = d_out.cpu().numpy()
     # e2e through the host-buffer entry point
     t0 = time.perf_counter()
@@ -406,6 +532,20 @@ def run_mr(a) -> None:
                          "sample": f"first {sample.size} candidates through verify_cpp.cpp is_prime_u64",
                          "matches_gpu": match},
         "gap_proofs": proofs,
+        "roofline": {"bound": "int", "achieved": (m_small + m_full) / t_meas / 1e9,
+                     "peak": (m_small + m_full) / t_ideal / 1e9, "unit": "G Montgomery products/s",
+                     "frac": t_ideal / t_meas, "traffic": None,
+                     "kernel": "mr_sieve_kernel + mr_finish_kernel (one call)", "kernel_ms": ms,
+                     "products_per_candidate": (m_small + m_full) / n.size,
+                     "products_small_modulus": m_small, "products_full_modulus": m_full,
+                     "peak_small_per_s": peak_small, "peak_full_per_s": peak_full,
+                     "peak_source": "voss_probe_mulmod: independent Montgomery squaring chains on this GPU in "
+                                    "this run (moduli < 2^63 and >= 2^63); peak = the products' time-weighted rate",
+                     "count_sample": int(msample.size),
+                     "traffic_note": "8 B read + 1 B written per candidate; mr_finish_kernel DRAM figures in "
+                                     "profiles/mr_finish_kernel_2e6.md"},
+        "clocks": clk,
+        "gpu_launches": 2 * a.steps,
     }
     print(json.dumps(out), flush=True)
 
@@ -516,7 +656,9 @@ def main():
             ctx.sieve_range_device(lo, hi, compat=True, seg_num=SEG_NUM, stream=stream.cuda_stream)
             ev[k][1].record(stream)
         stream.synchronize()
-        sieve_ms.append(ctx.last_kernel_ms()[0])
+        ph = ctx.last_phase_ms()
+        sieve_ms.append(ph[1])  # the tile kernel alone
+        step_kernels = ph[3]
     barrier()
     step_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
     kernel_ms = statistics.mean(sieve_ms)
@@ -586,7 +728,7 @@ def main():
                      "hbm_peak_measured_gbs": peaks.get("hbm_gbs"),
                      "traffic_source": tsrc},
         "clocks": clk,
-        "gpu_launches": 3 * a.steps,
+        "gpu_launches": step_kernels * a.steps,
         "result": {"pi": r.prime_count if r else None, "max_gap": r.max_gap if r else None,
                    "large_gaps": r.large_total if r else None},
     }

@@ -314,8 +314,20 @@ VOSS_API int voss_server_get_stats(voss_server* srv, voss_server_stats* out);
  * atomicAnd), measured by a bank-conflict-free kernel: the roofline denominator of the
  * shared-memory-bound sieve.  No counterpart in the reference. */
 VOSS_API int voss_probe_smem_rmw(voss_ctx* ctx, double* gbs);
-/* Kernel time (ms) of the last voss_sieve_range / _device call's sieve kernel, by CUDA events. */
+/* Montgomery products per second of this device (independent squaring chains, all lanes
+ * active, no memory traffic), for moduli of 64 bits (full) and below 2^63 (small): the roofline
+ * denominator of the Miller-Rabin kernels.  No counterpart in the reference. */
+VOSS_API int voss_probe_mulmod(voss_ctx* ctx, double* full_per_s, double* small_per_s);
+/* Device time (ms, CUDA events) of the last sieve launch on the context's events
+ * (voss_sieve_range[_device], voss_sieve_intervals, voss_gaps_at_least, voss_primes_range):
+ * sieve_ms from the launch's first device operation (descriptor copies, memsets) to the end of
+ * the tile kernel, total_ms to the end of its last kernel. */
 VOSS_API int voss_last_kernel_ms(const voss_ctx* ctx, double* sieve_ms, double* total_ms);
+/* The same launch in three consecutive phases: prepass_ms = descriptor copies, memsets and the
+ * large-prime pre-pass kernels; tile_ms = the tile kernel alone; tail_ms = the stitch, reduce and
+ * (intervals) finalize kernels; kernels = how many kernels the launch ran. */
+VOSS_API int voss_last_phase_ms(const voss_ctx* ctx, double* prepass_ms, double* tile_ms, double* tail_ms,
+                                uint32_t* kernels);
 
 #ifdef __cplusplus
 }

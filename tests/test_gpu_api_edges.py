@@ -46,3 +46,27 @@ def test_empty_and_tiny_ranges():
         assert ctx.prove_gaps(np.zeros(0, np.uint64), np.zeros(0, np.int32)).size == 0
         assert ctx.primes_range(10, 10).size == 0
         assert ctx.primes_range(1, 30).tolist() == [2, 3, 5, 7, 11, 13, 17, 19, 23, 29]
+
+
+def test_phase_times_and_kernel_counts():
+    """voss_last_phase_ms splits voss_last_kernel_ms into its phases and counts the kernels."""
+    with voss.Context(10**16 + 10**8) as ctx:
+        ctx.sieve_range(1, 10**9 + 1)
+        pre, tile, tail, k = ctx.last_phase_ms()
+        sieve, total = ctx.last_kernel_ms()
+        assert k == 3                                   # tile kernel, stitch, reduce (no pre-pass)
+        assert min(pre, tile, tail) >= 0 and tile > 0
+        assert abs(pre + tile - sieve) < 0.05 and abs(pre + tile + tail - total) < 0.05
+        lo = np.array([10**15, 10**12, 10**16], dtype=np.uint64)
+        hi = lo + np.array([10**7, 10**6, 10**8], dtype=np.uint64)
+        ctx.sieve_intervals(lo, hi)
+        pre, tile, tail, k = ctx.last_phase_ms()
+        assert k >= 5                                   # >= 1 pre-pass window + tile, stitch, reduce, finalize
+        assert pre > 0 and tile > 0 and tail > 0
+
+
+def test_mulmod_probe_rates():
+    with voss.Context(10**9) as ctx:
+        full, small = ctx.probe_mulmod()
+        assert 1e10 < full < 1e14 and 1e10 < small < 1e14
+        assert small >= 0.9 * full                      # the n < 2^63 product skips the carry checks

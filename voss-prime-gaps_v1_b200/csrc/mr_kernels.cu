@@ -242,6 +242,40 @@ __device__ __forceinline__ bool sprp_uniform(const Mont& M, uint64_t am, uint64_
   return ok;
 }
 
+// sprp_uniform for a base whose products are real multiplications, with 2-bit exponent digits:
+// x <- x^4 * a^digit for each digit of d from the top, a^0 = R, a, a^2, a^3 precomputed and
+// picked by selects (no memory).  A base then costs about 1.5 products per bit of d instead of
+// the 2 of the bitwise loop, which must multiply at every bit because some lane's bit is set.
+template <bool kSmallN>
+__device__ __forceinline__ bool sprp_uniform_w2(const Mont& M, uint64_t am, uint64_t d, int r, int top_w, int r_w) {
+  const uint64_t a2 = kSmallN ? mont_mul_small(am, am, M) : mont_mul(am, am, M);
+  const uint64_t a3 = kSmallN ? mont_mul_small(a2, am, M) : mont_mul(a2, am, M);
+  // an odd number of bits (top_w even) starts with the single top bit, then bit pairs (b, b - 1)
+  uint64_t x;
+  int b;
+  if ((top_w & 1) == 0) {
+    x = ((d >> top_w) & 1ull) ? am : M.one;
+    b = top_w - 1;
+  } else {
+    const uint32_t g = (uint32_t)(d >> (top_w - 1)) & 3u;
+    x = g == 0u ? M.one : (g == 1u ? am : (g == 2u ? a2 : a3));
+    b = top_w - 2;
+  }
+  for (; b >= 1; b -= 2) {
+    x = kSmallN ? mont_mul_small(x, x, M) : mont_mul(x, x, M);
+    x = kSmallN ? mont_mul_small(x, x, M) : mont_mul(x, x, M);
+    const uint32_t g = (uint32_t)(d >> (b - 1)) & 3u;
+    const uint64_t t = g == 0u ? M.one : (g == 1u ? am : (g == 2u ? a2 : a3));
+    x = kSmallN ? mont_mul_small(x, t, M) : mont_mul(x, t, M);
+  }
+  bool ok = (x == M.one) | (x == M.mone);
+  for (int j = 0; j < r_w - 1; ++j) {
+    x = kSmallN ? mont_mul_small(x, x, M) : mont_mul(x, x, M);
+    ok |= (j < r - 1) & (x == M.mone);
+  }
+  return ok;
+}
+
 // Bases 3, 5, 7, ... of mr_finish_kernel for one warp: each lane stops after bases_needed(n)
 // bases or its first failure; the warp stops when no lane wants another base.
 template <bool kSmallN>
@@ -249,7 +283,7 @@ __device__ __forceinline__ bool sprp_bases_3_on(const Mont& M, uint64_t d, int r
   const uint64_t n_ = M.n;
   const uint64_t r1 = M.one, r2 = mod_add(r1, r1, n_), r4 = mod_add(r2, r2, n_), r6 = mod_add(r4, r2, n_);
   uint64_t a = mod_add(r2, r1, n_);  // 3R: bases 3,5,7,11,13,17,19,23,29,31,37 by their gaps
-  bool prime = sprp_uniform<kSmallN>(M, a, d, r, top_w, r_w, false);
+  bool prime = sprp_uniform_w2<kSmallN>(M, a, d, r, top_w, r_w);
 #pragma unroll 1
   for (int s = 0; s < 10; ++s) {
     // base index s + 2 (5, 7, 11, ...): still wanted by a lane that is prime so far and needs it
@@ -257,7 +291,7 @@ __device__ __forceinline__ bool sprp_bases_3_on(const Mont& M, uint64_t d, int r
     if (!__any_sync(0xFFFFFFFFu, want)) break;
     const int step = (0x6264242422ull >> (4 * s)) & 0xF;  // 2,2,4,2,4,2,4,6,2,6
     a = mod_add(a, step == 2 ? r2 : (step == 4 ? r4 : r6), n_);
-    const bool pass = sprp_uniform<kSmallN>(M, a, d, r, top_w, r_w, false);
+    const bool pass = sprp_uniform_w2<kSmallN>(M, a, d, r, top_w, r_w);
     prime = want ? pass : prime;
   }
   return prime;
@@ -447,6 +481,73 @@ int launch_prove_gaps(const uint64_t* d_p_after, const int32_t* d_gap, uint64_t 
   const int grid = (int)(want < (uint64_t)sm_count * 8 ? want : (uint64_t)sm_count * 8);
   prove_interior_kernel<<<grid, kProveBlock, 0, s>>>(d_p_after, d_gap, count, d_ends_ok, d_ok);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// Peak rate of the Montgomery product on this device: independent squaring chains, every lane
+// active, no branches and no memory traffic.  The roofline denominator of the Miller-Rabin
+// kernels, which spend their time in the same products (one figure per variant: moduli below
+// and above 2^63).
+constexpr int kMulmodChains = 8;
+constexpr int kMulmodIters = 2048;
+constexpr int kMulmodBlock = 256;
+
+template <bool kSmallN>
+__global__ void __launch_bounds__(kMulmodBlock) mulmod_probe_kernel(uint64_t nbase, uint64_t* sink) {
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t n = nbase | (tid << 1) | 1ull;  // an odd modulus per thread
+  const Mont M = mont_setup(n);
+  uint64_t x[kMulmodChains];
+#pragma unroll
+  for (int c = 0; c < kMulmodChains; ++c) x[c] = (M.one >> 1) + (uint64_t)c + 1ull;  // < n
+#pragma unroll 1
+  for (int i = 0; i < kMulmodIters; ++i) {
+#pragma unroll
+    for (int c = 0; c < kMulmodChains; ++c) x[c] = kSmallN ? mont_mul_small(x[c], x[c], M) : mont_mul(x[c], x[c], M);
+  }
+  uint64_t acc = 0;
+#pragma unroll
+  for (int c = 0; c < kMulmodChains; ++c) acc ^= x[c];
+  if (acc == 1ull) sink[0] = acc;  // keeps the chains live; practically never taken
+}
+
+template <bool kSmallN>
+static int probe_mulmod_one(int sm_count, cudaStream_t s, uint64_t* sink, double* per_s) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mulmod_probe_kernel<kSmallN>, kMulmodBlock, 0) !=
+          cudaSuccess ||
+      occ < 1)
+    return -1;
+  const int grid = sm_count * occ;  // one full wave
+  const uint64_t nbase = kSmallN ? (1ull << 62) : (3ull << 62);
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return -1;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return -1;
+  }
+  mulmod_probe_kernel<kSmallN><<<grid, kMulmodBlock, 0, s>>>(nbase, sink);  // warm-up
+  const int reps = 3;
+  cudaEventRecord(e0, s);
+  for (int r = 0; r < reps; ++r) mulmod_probe_kernel<kSmallN><<<grid, kMulmodBlock, 0, s>>>(nbase, sink);
+  cudaEventRecord(e1, s);
+  const cudaError_t st = cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != cudaSuccess || ms <= 0) return -1;
+  *per_s = (double)grid * kMulmodBlock * kMulmodChains * kMulmodIters * reps / (ms * 1e-3);
+  return 0;
+}
+
+int probe_mulmod(int sm_count, void* stream, double* full_per_s, double* small_per_s) {
+  cudaStream_t s = (cudaStream_t)stream;
+  uint64_t* sink = nullptr;
+  if (cudaMalloc(&sink, sizeof(uint64_t)) != cudaSuccess) return -1;
+  int rc = probe_mulmod_one<false>(sm_count, s, sink, full_per_s);
+  if (rc == 0) rc = probe_mulmod_one<true>(sm_count, s, sink, small_per_s);
+  cudaFree(sink);
+  return rc;
 }
 
 }  // namespace voss

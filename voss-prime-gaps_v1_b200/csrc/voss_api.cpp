@@ -184,9 +184,6 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
   const uint64_t cap = want_large ? std::min(std::max(large_cap, (uint64_t)1), kMaxLargeCap) : 1;
   if ((rc = W.large.ensure(sizeof(LargeGapDev) * cap))) return rc;
   if ((rc = W.large_iv.ensure(sizeof(uint32_t) * cap))) return rc;
-  if (n_iv) CUDA_TRY(cudaMemcpyAsync(W.iv.p, P.iv.data(), sizeof(IntervalDev) * n_iv, cudaMemcpyHostToDevice, s));
-  if (!emit) CUDA_TRY(cudaMemsetAsync(W.acc.p, 0, sizeof(unsigned long long) * kAccStride * std::max<size_t>(1, n_iv), s));
-  CUDA_TRY(cudaMemsetAsync(W.counters.p, 0, sizeof(uint32_t) * kCtrWords, s));
 
   SieveArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -275,16 +272,24 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
       w.j1 = (uint32_t)(std::upper_bound(c->primes.begin(), c->primes.end(), sc[w.off].sqrt_hi) - c->primes.begin());
     }
     if ((rc = W.gbm.ensure(gbm_bytes)) || (rc = W.scat.ensure(sizeof(IntervalScatter) * sc.size()))) return rc;
-    CUDA_TRY(cudaMemsetAsync(W.gbm.p, 0xFF, gbm_bytes, s));
-    CUDA_TRY(cudaMemcpyAsync(W.scat.p, sc.data(), sizeof(IntervalScatter) * sc.size(), cudaMemcpyHostToDevice, s));
     a.gbm = W.gbm.as<uint32_t>();
     a.scatter_first = j0;
   }
+  // Device work of the launch, all of it after ev0 (the host planning above is done first, so
+  // the GPU never waits on the host inside the events).
   CUDA_TRY(cudaEventRecord(E.ev0, s));
+  if (n_iv) CUDA_TRY(cudaMemcpyAsync(W.iv.p, P.iv.data(), sizeof(IntervalDev) * n_iv, cudaMemcpyHostToDevice, s));
+  if (!emit) CUDA_TRY(cudaMemsetAsync(W.acc.p, 0, sizeof(unsigned long long) * kAccStride * std::max<size_t>(1, n_iv), s));
+  CUDA_TRY(cudaMemsetAsync(W.counters.p, 0, sizeof(uint32_t) * kCtrWords, s));
+  if (scatter) {
+    CUDA_TRY(cudaMemsetAsync(W.gbm.p, 0xFF, gbm_bytes, s));
+    CUDA_TRY(cudaMemcpyAsync(W.scat.p, sc.data(), sizeof(IntervalScatter) * sc.size(), cudaMemcpyHostToDevice, s));
+  }
   for (const Window& w : wins)
     if (launch_scatter_large(a.primes, a.magic, j0, w.j1, W.scat.as<IntervalScatter>() + w.off, w.n,
                              W.gbm.as<uint32_t>(), c->sm_count, s))
       return fail(VOSS_ERR_CUDA, "large-prime pre-pass launch failed");
+  if (E.evp) CUDA_TRY(cudaEventRecord(E.evp, s));
   if (P.n_tiles) {
     int lr = emit ? launch_sieve_emit(a, grid, (int)c->tune.block_threads, smem, s)
                   : launch_sieve_stats(a, grid, (int)c->tune.block_threads, smem, s);
@@ -296,6 +301,7 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
     if (launch_reduce(a, W.out.as<IntervalOut>(), s)) return fail(VOSS_ERR_CUDA, "reduce launch failed");
   }
   CUDA_TRY(cudaEventRecord(E.ev2, s));
+  c->last_kernels = (uint32_t)wins.size() + (P.n_tiles ? 1u : 0u) + (emit ? 0u : 2u);
   if (args_out) *args_out = a;
   return VOSS_OK;
 }
@@ -304,6 +310,7 @@ int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_c
                 uint32_t min_gap = 0, SieveArgs* args_out = nullptr) {
   LaunchEvents E;
   E.ev0 = c->ev0;
+  E.evp = c->evp;
   E.ev1 = c->ev1;
   E.ev2 = c->ev2;
   return launch_plan_ws(c, c->ws, E, P, want_large, large_cap, emit, s, min_gap, args_out);
@@ -609,7 +616,7 @@ VOSS_API int voss_ctx_create(int device, uint64_t max_hi, voss_ctx** out) {
       cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_copy, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaEventCreate(&c->ev2) != cudaSuccess)
+      cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->evp) != cudaSuccess)
     return bail(fail(VOSS_ERR_CUDA, "stream/event creation failed"));
   c->primes = base_primes(isqrt_u64(max_hi - 1));
   const size_t np = std::max<size_t>(1, c->primes.size());
@@ -641,6 +648,7 @@ VOSS_API void voss_ctx_destroy(voss_ctx* c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
+  if (c->evp) cudaEventDestroy(c->evp);
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->ev_copy) cudaEventDestroy(c->ev_copy);
@@ -723,6 +731,23 @@ VOSS_API int voss_last_kernel_ms(const voss_ctx* c, double* sieve_ms, double* to
   return VOSS_OK;
 }
 
+VOSS_API int voss_last_phase_ms(const voss_ctx* c, double* prepass_ms, double* tile_ms, double* tail_ms,
+                                uint32_t* kernels) {
+  NvtxRange nvtx_("voss_last_phase_ms");
+  if (!c) return fail(VOSS_ERR_ARG, "ctx is NULL");
+  cudaSetDevice(c->device);
+  float a = 0, b = 0, t = 0;
+  CUDA_TRY(cudaEventSynchronize(c->ev2));
+  CUDA_TRY(cudaEventElapsedTime(&a, c->ev0, c->evp));
+  CUDA_TRY(cudaEventElapsedTime(&b, c->evp, c->ev1));
+  CUDA_TRY(cudaEventElapsedTime(&t, c->ev1, c->ev2));
+  if (prepass_ms) *prepass_ms = a;
+  if (tile_ms) *tile_ms = b;
+  if (tail_ms) *tail_ms = t;
+  if (kernels) *kernels = c->last_kernels;
+  return VOSS_OK;
+}
+
 VOSS_API int voss_sieve_intervals(voss_ctx* c, const uint64_t* lo, const uint64_t* hi, uint32_t n,
                                   voss_interval_stats* out) {
   NvtxRange nvtx_("voss_sieve_intervals");
@@ -742,6 +767,8 @@ VOSS_API int voss_sieve_intervals(voss_ctx* c, const uint64_t* lo, const uint64_
   if ((rc = c->ws.istats.ensure(sizeof(voss_interval_stats) * n))) return rc;
   if (launch_interval_finalize(a, c->ws.out.as<IntervalOut>(), c->ws.istats.as<voss_interval_stats>(), c->stream))
     return fail(VOSS_ERR_CUDA, "interval finalize launch failed");
+  CUDA_TRY(cudaEventRecord(c->ev2, c->stream));  // the finalize kernel counts in the launch's time
+  c->last_kernels += 1;
   uint32_t ctr[kCtrWords];
   CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaMemcpyAsync(out, c->ws.istats.p, sizeof(voss_interval_stats) * n, cudaMemcpyDeviceToHost, c->stream));
@@ -914,6 +941,13 @@ VOSS_API int voss_probe_smem_rmw(voss_ctx* c, double* gbs) {
   double bytes = 0;
   if (probe_smem_rmw(c->sm_count, c->stream, &ms, &bytes)) return fail(VOSS_ERR_CUDA, "probe failed");
   *gbs = bytes / (ms * 1e-3) / 1e9;
+  return VOSS_OK;
+}
+
+VOSS_API int voss_probe_mulmod(voss_ctx* c, double* full_per_s, double* small_per_s) {
+  if (!c || !full_per_s || !small_per_s) return fail(VOSS_ERR_ARG, "NULL argument");
+  cudaSetDevice(c->device);
+  if (probe_mulmod(c->sm_count, c->stream, full_per_s, small_per_s)) return fail(VOSS_ERR_CUDA, "probe failed");
   return VOSS_OK;
 }
 

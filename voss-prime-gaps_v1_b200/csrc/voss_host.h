@@ -74,10 +74,11 @@ struct Workspace {
   bool gbm_fixed = false;
 };
 
-// Events bracketing one launch: ev0 before the sieve kernel, ev1 after it, ev2 after the
-// stitch/reduce kernels.
+// Events bracketing one launch: ev0 before all of its device work (descriptor copies, memsets),
+// ev1 after the tile kernel, ev2 after the stitch/reduce kernels; evp (optional) after the
+// large-prime pre-pass, just before the tile kernel.
 struct LaunchEvents {
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, evp = nullptr;
 };
 
 struct RunPlan {
@@ -104,7 +105,7 @@ struct voss_ctx {
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream = nullptr;  // host-to-device copies overlapped with work on `stream`
   cudaEvent_t ev_copy = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, evp = nullptr;
   uint64_t max_hi = 0;
   std::vector<uint32_t> primes;  // >= 37
   voss_host::DevBuf d_primes, d_magic, d_pretab;
@@ -118,6 +119,7 @@ struct voss_ctx {
   uint32_t r_tiles = 0;
   uint64_t r_large_cap = 0;
   float sieve_ms = 0, total_ms = 0;
+  uint32_t last_kernels = 0;  // kernels of the last launch_plan_ws (+ finalize for intervals)
   // host side of the large-gap list: pinned, grow-only staging for the device-to-host copy of
   // the list (sorted on the device), so that repeated calls touch no fresh pages
   voss_large_gap* h_large = nullptr;

@@ -177,5 +177,7 @@ int launch_mr(const uint64_t* d_n, uint64_t count, uint8_t* d_out, uint32_t* d_w
 int launch_prove_gaps(const uint64_t* d_p_after, const int32_t* d_gap, uint64_t count, uint8_t* d_ok,
                       uint64_t* d_ends, uint8_t* d_ends_ok, uint32_t* d_work, uint32_t* d_nwork, void* stream,
                       int sm_count);
+// Montgomery products per second of independent squaring chains (moduli above / below 2^63).
+int probe_mulmod(int sm_count, void* stream, double* full_per_s, double* small_per_s);
 
 }  // namespace voss

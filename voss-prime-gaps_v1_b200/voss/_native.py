@@ -134,6 +134,9 @@ SIGNATURES = {
     "voss_server_get_stats": (c_int, [c_void_p, POINTER(ServerStats)]),
     "voss_probe_smem_rmw": (c_int, [c_void_p, POINTER(c_double)]),
     "voss_last_kernel_ms": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
+    "voss_last_phase_ms": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double), POINTER(c_double),
+                                   POINTER(c_uint32)]),
+    "voss_probe_mulmod": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
 }
 
 _lib = None

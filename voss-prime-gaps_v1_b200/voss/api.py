@@ -6,7 +6,7 @@ Every method calls straight into the C ABI; nothing here computes primes itself.
 from __future__ import annotations
 
 import ctypes
-from ctypes import byref, c_double, c_int, c_uint64, c_void_p
+from ctypes import byref, c_double, c_int, c_uint32, c_uint64, c_void_p
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -159,6 +159,13 @@ class Context:
         N.check(self.lib.voss_last_kernel_ms(self._h, byref(a), byref(b)))
         return a.value, b.value
 
+    def last_phase_ms(self) -> tuple[float, float, float, int]:
+        """(pre-pass incl. copies and memsets, tile kernel, stitch/reduce/finalize) in ms of the
+        last launch, and the number of kernels it launched."""
+        a, b, t, k = c_double(), c_double(), c_double(), c_uint32()
+        N.check(self.lib.voss_last_phase_ms(self._h, byref(a), byref(b), byref(t), byref(k)))
+        return a.value, b.value, t.value, k.value
+
     def primes_range(self, lo: int, hi: int, cap: int | None = None) -> np.ndarray:
         cnt = c_uint64()
         if cap is None:
@@ -250,6 +257,12 @@ class Context:
         g = c_double()
         N.check(self.lib.voss_probe_smem_rmw(self._h, byref(g)))
         return g.value
+
+    def probe_mulmod(self) -> tuple[float, float]:
+        """Montgomery products/s of this device for 64-bit moduli and for moduli below 2^63."""
+        f, s = c_double(), c_double()
+        N.check(self.lib.voss_probe_mulmod(self._h, byref(f), byref(s)))
+        return f.value, s.value
 
 
 def write_artifacts(res: RangeResult, out_dir: str) -> None:

@@ -301,7 +301,8 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
     if (launch_reduce(a, W.out.as<IntervalOut>(), s)) return fail(VOSS_ERR_CUDA, "reduce launch failed");
   }
   CUDA_TRY(cudaEventRecord(E.ev2, s));
-  c->last_kernels = (uint32_t)wins.size() + (P.n_tiles ? 1u : 0u) + (emit ? 0u : 2u);
+  if (&W == &c->ws)  // the context's own launches (server slots keep their own workspaces)
+    c->last_kernels = (uint32_t)wins.size() + (P.n_tiles ? 1u : 0u) + (emit ? 0u : 2u);
   if (args_out) *args_out = a;
   return VOSS_OK;
 }

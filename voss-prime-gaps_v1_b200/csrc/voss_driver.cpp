@@ -33,7 +33,7 @@ int count_tiles(voss_ctx* c, uint64_t lo, uint64_t hi, RunPlan* P, std::vector<u
   if (a >= hi) return VOSS_OK;
   int rc = plan_intervals(c, &a, &hi, 1, 0, P);
   if (rc) return rc;
-  LaunchEvents E{c->ev0, c->ev1, c->ev2};
+  LaunchEvents E{c->ev0, c->ev1, c->ev2, c->evp};
   rc = launch_plan_ws(c, c->ws, E, *P, false, 0, false, s, 0, nullptr);
   if (rc) return rc;
   std::vector<TilePartial> parts(P->n_tiles);
@@ -74,7 +74,7 @@ int emit_window(voss_ctx* c, const RunPlan& P, const std::vector<uint64_t>& pref
       (rc = c->ws.emit.ensure(sizeof(unsigned long long) * n)))
     return rc;
   CUDA_TRY(cudaMemcpyAsync(c->ws.offsets.p, offs.data(), sizeof(unsigned long long) * Q.n_tiles, cudaMemcpyHostToDevice, s));
-  LaunchEvents E{c->ev0, c->ev1, c->ev2};
+  LaunchEvents E{c->ev0, c->ev1, c->ev2, c->evp};
   rc = launch_plan_ws(c, c->ws, E, Q, false, 0, true, s, 0, nullptr);
   if (rc) return rc;
   out->resize(n);

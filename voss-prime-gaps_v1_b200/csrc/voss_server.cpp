@@ -9,7 +9,10 @@
 // batch: one persistent tile-kernel launch over all the batch's (interval, tile) work items,
 // then one Miller-Rabin launch over all its candidates.  Requests that arrive while batches run
 // are admitted into the next slot that frees up, so batches overlap on the device.  A slot's
-// completion is signalled by a host function queued behind its last copy; every wait is bounded.
+// completion is an event recorded behind its last copy, which the scheduler polls while batches
+// are in flight (it sleeps on a condition variable only when the server is idle); every wait is
+// bounded.
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -50,7 +53,8 @@ struct Slot {
   Workspace ws;
   LaunchEvents E;
   bool busy = false;
-  bool ready = false;  // set by the completion host function
+  bool ready = false;            // the batch's work (or its failed launch) is finished
+  cudaEvent_t done = nullptr;    // recorded behind the batch's last copy
   std::vector<Request*> iv, mr;
   uint32_t n_iv = 0;
   uint64_t n_mr = 0;
@@ -71,6 +75,7 @@ struct voss_server {
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Request*> pending;
+  std::atomic<uint64_t> submitted{0};  // requests ever enqueued: the polling scheduler's wake-up
   std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
   uint64_t next_id = 1;
   bool stop = false;
@@ -97,14 +102,16 @@ uint32_t tiles_of(const voss_ctx* c, uint64_t lo, uint64_t hi) {
   return t > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)t;
 }
 
-void CUDART_CB on_slot_done(void* p) {
-  Slot* sl = static_cast<Slot*>(p);
-  voss_server* S = sl->owner;
-  {
-    std::lock_guard<std::mutex> lk(S->mu);
-    sl->ready = true;
+// Poll a busy slot's completion event: true once its work is done (or the query failed, which
+// fails the batch).
+bool slot_finished(Slot& sl) {
+  const cudaError_t e = cudaEventQuery(sl.done);
+  if (e == cudaErrorNotReady) return false;
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    sl.launch_error = fail(VOSS_ERR_CUDA, "batch completion query failed: %s", cudaGetErrorString(e));
   }
-  S->cv_work.notify_one();
+  return true;
 }
 
 // Queue one batch on a free slot (called without the server lock; the batch lists are owned by
@@ -151,7 +158,7 @@ int launch_batch(voss_server* S, Slot& sl) {
     CUDA_TRY(cudaMemcpyAsync(sl.h_mr_out, sl.ws.mr_out.p, sl.n_mr, cudaMemcpyDeviceToHost, s));
     S->launches += 2;
   }
-  CUDA_TRY(cudaLaunchHostFunc(s, on_slot_done, &sl));
+  CUDA_TRY(cudaEventRecord(sl.done, s));
   return VOSS_OK;
 }
 
@@ -222,7 +229,7 @@ void scheduler(voss_server* S) {
   std::unique_lock<std::mutex> lk(S->mu);
   for (;;) {
     for (auto& up : S->slots)
-      if (up->busy && up->ready) complete_slot(S, *up);
+      if (up->busy && (up->ready || slot_finished(*up))) complete_slot(S, *up);
     if (S->stop && S->pending.empty() && S->inflight == 0) break;
     bool launched = false;
     for (auto& up : S->slots) {
@@ -248,7 +255,23 @@ void scheduler(voss_server* S) {
       launched = true;
     }
     if (launched) continue;
-    // bounded wait: woken by submissions and slot completions; the timeout is a safety net
+    if (S->inflight > 0) {
+      // batches on the GPU: poll their completion events (and new submissions) instead of
+      // sleeping, so a finished batch is delivered within microseconds rather than after a
+      // driver callback thread and a condition-variable wake-up
+      const uint64_t seen = S->submitted.load(std::memory_order_acquire);
+      lk.unlock();
+      for (;;) {
+        bool any = false;
+        for (auto& up : S->slots)
+          if (up->busy && !up->ready && cudaEventQuery(up->done) != cudaErrorNotReady) any = true;
+        if (any || S->submitted.load(std::memory_order_acquire) != seen) break;
+        std::this_thread::yield();
+      }
+      lk.lock();
+      continue;
+    }
+    // idle: woken by submissions; the timeout is a safety net
     S->cv_work.wait_for(lk, std::chrono::milliseconds(2));
   }
 }
@@ -265,7 +288,8 @@ Slot* make_slot(voss_server* S, int* rc) {
   };
   if (cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&sl->E.ev0) != cudaSuccess || cudaEventCreate(&sl->E.ev1) != cudaSuccess ||
-      cudaEventCreate(&sl->E.ev2) != cudaSuccess)
+      cudaEventCreate(&sl->E.ev2) != cudaSuccess ||
+      cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming) != cudaSuccess)
     return bad(fail(VOSS_ERR_CUDA, "server slot stream/event creation failed"));
   Workspace& W = sl->ws;
   int e;
@@ -302,6 +326,7 @@ void free_slot(Slot* sl) {
   if (sl->E.ev0) cudaEventDestroy(sl->E.ev0);
   if (sl->E.ev1) cudaEventDestroy(sl->E.ev1);
   if (sl->E.ev2) cudaEventDestroy(sl->E.ev2);
+  if (sl->done) cudaEventDestroy(sl->done);
   if (sl->stream) cudaStreamDestroy(sl->stream);
   delete sl;
 }
@@ -319,6 +344,7 @@ uint64_t enqueue(voss_server* S, std::unique_ptr<Request> r) {
     raw->t_submit = Clock::now();
     S->reqs.emplace(raw->id, std::move(r));
     S->pending.push_back(raw);
+    S->submitted.fetch_add(1, std::memory_order_release);
   }
   S->cv_work.notify_one();
   return raw->id;

@@ -121,7 +121,9 @@ typedef struct voss_tuning {
   uint32_t medium_mode;     /* other primes: 0 = a thread per prime, 1 = a lane per (prime, residue) */
   uint32_t walk_sixteenths; /* mode 0: primes p >= walk_sixteenths*tile_bytes/16 walk their coprime
                                multiples instead of 8 residue progressions (>= 16*mult_factor: never) */
-  uint32_t reserved[1];
+  uint32_t mr_route;        /* voss_sieve_intervals: an interval whose base primes >= mult_factor*tile_bytes
+                               outnumber mr_route times its length is tested by Miller-Rabin instead of
+                               sieved (0 = default 50; 0xFFFFFFFF = never) */
 } voss_tuning;
 
 typedef struct voss_ctx voss_ctx;

@@ -188,3 +188,37 @@ def test_sharded_ranges_merge_to_the_whole(gpu_ctx, compat):
     m2 = voss.merge_stats(shards)
     assert sorted(zip(m2.large["position"].tolist(), m2.large["gap"].tolist())) == \
         sorted(zip(whole.large["position"].tolist(), whole.large["gap"].tolist()))
+
+
+def _same_intervals(a, b):
+    for f in ("lo", "hi", "prime_count", "first_prime", "last_prime", "max_gap", "max_gap_lo", "gap_overflow"):
+        np.testing.assert_array_equal(a[f], b[f], err_msg=f)
+    np.testing.assert_array_equal(a["gap_hist"], b["gap_hist"])
+
+
+def test_short_intervals_by_miller_rabin_equal_the_sieve(gpu_ctx_big):
+    """Short intervals at high starts go to the Miller-Rabin path (short_iv.cu); with the route
+    switched off the same batch is sieved.  Both must agree bit for bit, for a mixed batch, a
+    batch routed entirely, intervals without wheel integers, and against the oracle."""
+    rng = np.random.default_rng(11)
+    k = 96
+    lo = (10 ** rng.uniform(9, 18, k)).astype(np.uint64)
+    ln = (10 ** rng.uniform(0, 6, k)).astype(np.uint64)
+    base = 30 * (10**16 // 30)
+    lo[:4] = [base + 2, base + 1, 10**18 - 10**4, 3 * 10**17 + 11]
+    ln[:4] = [5, 1, 10**4, 3]                       # no wheel integer; only base + 1; ...
+    hi = lo + ln
+    t0 = gpu_ctx_big.tuning()
+    try:
+        routed = gpu_ctx_big.sieve_intervals(lo, hi)
+        gpu_ctx_big.set_tuning(**{**t0, "mr_route": 0xFFFFFFFF})
+        sieved = gpu_ctx_big.sieve_intervals(lo, hi)
+        _same_intervals(routed, sieved)
+        gpu_ctx_big.set_tuning(**t0)
+        only = gpu_ctx_big.sieve_intervals(lo[:4], hi[:4])      # every interval routed: no sieve launch
+        assert gpu_ctx_big.last_phase_ms()[3] == 4              # candidates, two Miller-Rabin kernels, statistics
+        _same_intervals(only, sieved[:4])
+    finally:
+        gpu_ctx_big.set_tuning(**t0)
+    sel = np.nonzero(hi < 10**16)[0][:16]
+    _same_intervals(routed[sel], O.sieve_intervals(lo[sel], hi[sel]))

@@ -895,11 +895,12 @@ __global__ void reduce_kernel(SieveArgs a, IntervalOut* out) {
 // One block per interval: fold the accumulators into voss_interval_stats on the device, so
 // that only the result (not the raw counters) crosses to the host.  lo/hi and the primes
 // 2, 3, 5 are filled in on the host.
-__global__ void interval_finalize_kernel(SieveArgs a, const IntervalOut* io, voss_interval_stats* out) {
+__global__ void interval_finalize_kernel(SieveArgs a, const IntervalOut* io, voss_interval_stats* out,
+                                         const uint32_t* out_index) {
   const uint32_t ivx = blockIdx.x;
   if (ivx >= a.n_intervals) return;
   const unsigned long long* A = a.acc + (size_t)ivx * kAccStride;
-  voss_interval_stats* s = out + ivx;
+  voss_interval_stats* s = out + (out_index ? out_index[ivx] : ivx);
   for (uint32_t b = threadIdx.x; b < (uint32_t)VOSS_IHIST; b += blockDim.x) {
     unsigned long long v = 0;
     if (b > 0) {
@@ -921,9 +922,10 @@ __global__ void interval_finalize_kernel(SieveArgs a, const IntervalOut* io, vos
   }
 }
 
-int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_interval_stats* out, void* stream) {
+int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_interval_stats* out,
+                             const uint32_t* out_index, void* stream) {
   if (a.n_intervals == 0) return 0;
-  interval_finalize_kernel<<<a.n_intervals, 256, 0, (cudaStream_t)stream>>>(a, io, out);
+  interval_finalize_kernel<<<a.n_intervals, 256, 0, (cudaStream_t)stream>>>(a, io, out, out_index);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

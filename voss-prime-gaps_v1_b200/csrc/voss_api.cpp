@@ -54,6 +54,11 @@ int DevBuf::ensure(size_t need) {
 const int kW30[8] = {1, 7, 11, 13, 17, 19, 23, 29};
 const int kQ[VOSS_NUM_Q] = VOSS_Q_LIST;
 
+// Wheel integers (coprime to 30) below x within its block of 30, and below x in all.
+constexpr uint8_t kCoprime30Below[30] = {0, 0, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 3, 3, 4,
+                                         4, 4, 4, 5, 5, 6, 6, 6, 6, 7, 7, 7, 7, 7, 7};
+uint64_t wheel_count_below(uint64_t x) { return 8ull * (x / 30) + kCoprime30Below[x % 30]; }
+
 uint64_t isqrt_u64(uint64_t x) {
   uint64_t s = (uint64_t)std::sqrt((long double)x);
   while (s * s > x) --s;
@@ -114,6 +119,7 @@ int apply_tuning(voss_ctx* c, const voss_tuning& t0) {
   if (!t.coop_div) t.coop_div = 128;
   if (!t.mult_factor) t.mult_factor = 8;
   if (!t.walk_sixteenths) t.walk_sixteenths = 4;
+  if (!t.mr_route) t.mr_route = 50;
   if (t.block_threads != 512 && t.block_threads != 1024)
     return fail(VOSS_ERR_ARG, "block_threads must be 512 or 1024");
   if (t.medium_mode > 1) return fail(VOSS_ERR_ARG, "medium_mode must be 0 or 1");
@@ -315,6 +321,92 @@ int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_c
   E.ev1 = c->ev1;
   E.ev2 = c->ev2;
   return launch_plan_ws(c, c->ws, E, P, want_large, large_cap, emit, s, min_gap, args_out);
+}
+
+// Route a batch of intervals (see voss_host.h) and launch it.
+void route_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, uint32_t n, uint64_t cand_cap,
+                     IntervalRoute* R) {
+  NvtxRange r("route");
+  // An interval whose base primes at or above the large-prime threshold outnumber mr_route
+  // times its length costs more in per-prime reductions than Miller-Rabin of its wheel integers
+  // (about 30 Montgomery products per integer) costs; it goes to short_iv.cu.
+  const uint64_t p_large = (uint64_t)c->tune.mult_factor * 4ull * c->tune.block_threads * c->tune.chunk_words;
+  const size_t jl = (size_t)(std::lower_bound(c->primes.begin(), c->primes.end(),
+                                              (uint32_t)std::min<uint64_t>(p_large, 0xFFFFFFFFull)) -
+                             c->primes.begin());
+  const uint64_t route = c->tune.mr_route;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint64_t a = std::max<uint64_t>(lo[i], 7);
+    bool mr = false;
+    if (route != 0xFFFFFFFFull && a < hi[i]) {
+      const uint64_t sq = isqrt_u64(hi[i] - 1);
+      const size_t np = (size_t)(std::upper_bound(c->primes.begin(), c->primes.end(),
+                                                  (uint32_t)std::min<uint64_t>(sq, 0xFFFFFFFFull)) -
+                                 c->primes.begin());
+      const uint64_t pairs = np > jl ? np - jl : 0;
+      const uint64_t len = hi[i] - a;
+      mr = len < (1ull << 31) && pairs / route > len && R->n_cand + len <= cand_cap;
+    }
+    if (mr) {
+      ShortInterval I;
+      I.base = 30ull * (a / 30);
+      I.cand_off = R->n_cand;
+      I.j0 = (uint32_t)kCoprime30Below[a % 30];
+      I.n_cand = (uint32_t)(wheel_count_below(hi[i]) - wheel_count_below(a));
+      I.out_index = i;
+      I.pad = 0;
+      R->n_cand += I.n_cand;
+      R->sv.push_back(I);
+    } else {
+      R->lo.push_back(lo[i]);
+      R->hi.push_back(hi[i]);
+      R->map.push_back(i);
+    }
+  }
+}
+
+int launch_routed(voss_ctx* c, Workspace& W, const LaunchEvents& E, const IntervalRoute& R, uint32_t n,
+                  cudaStream_t s, uint32_t* kernels) {
+  int rc;
+  uint32_t k = 0;
+  if (!R.lo.empty()) {
+    RunPlan P;
+    if ((rc = plan_intervals(c, R.lo.data(), R.hi.data(), (uint32_t)R.lo.size(), 0, &P))) return rc;
+    SieveArgs a;
+    if ((rc = launch_plan_ws(c, W, E, P, false, 0, false, s, 0, &a))) return rc;
+    k = (uint32_t)(&W == &c->ws ? c->last_kernels : 3) + 1;
+    const bool identity = R.lo.size() == n;
+    if (!identity) {
+      if ((rc = W.sh_map.ensure(sizeof(uint32_t) * R.map.size()))) return rc;
+      CUDA_TRY(cudaMemcpyAsync(W.sh_map.p, R.map.data(), sizeof(uint32_t) * R.map.size(), cudaMemcpyHostToDevice, s));
+    }
+    if (launch_interval_finalize(a, W.out.as<IntervalOut>(), W.istats.as<voss_interval_stats>(),
+                                 identity ? nullptr : W.sh_map.as<uint32_t>(), s))
+      return fail(VOSS_ERR_CUDA, "interval finalize launch failed");
+  } else {
+    // no sieve launch: the events bracket the Miller-Rabin path alone
+    if ((rc = W.counters.ensure(sizeof(uint32_t) * kCtrWords))) return rc;
+    for (cudaEvent_t e : {E.ev0, E.evp, E.ev1})
+      if (e) CUDA_TRY(cudaEventRecord(e, s));
+    CUDA_TRY(cudaMemsetAsync(W.counters.p, 0, sizeof(uint32_t) * kCtrWords, s));
+  }
+  if (!R.sv.empty()) {
+    NvtxRange r("short intervals by Miller-Rabin");
+    const uint64_t nc = R.n_cand;
+    if ((rc = W.sh_iv.ensure(sizeof(ShortInterval) * R.sv.size())) || (rc = W.mr_in.ensure(8 * std::max<uint64_t>(nc, 1))) ||
+        (rc = W.mr_out.ensure(std::max<uint64_t>(nc, 1))) || (rc = W.mr_work.ensure(sizeof(uint32_t) * (nc + 8))))
+      return rc;
+    CUDA_TRY(cudaMemcpyAsync(W.sh_iv.p, R.sv.data(), sizeof(ShortInterval) * R.sv.size(), cudaMemcpyHostToDevice, s));
+    uint32_t* work = W.mr_work.as<uint32_t>();
+    if (launch_short_intervals(W.sh_iv.as<ShortInterval>(), (uint32_t)R.sv.size(), nc, W.mr_in.as<uint64_t>(),
+                               W.mr_out.as<uint8_t>(), work + 8, work, W.istats.as<voss_interval_stats>(), c->sm_count,
+                               s))
+      return fail(VOSS_ERR_CUDA, "short-interval launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    k += nc ? 4 : 1;
+  }
+  if (E.ev2) CUDA_TRY(cudaEventRecord(E.ev2, s));  // finalize and the Miller-Rabin path count in the launch's time
+  if (kernels) *kernels = k;
+  return VOSS_OK;
 }
 
 int check_device_error(const uint32_t* ctr_host) {
@@ -759,21 +851,24 @@ VOSS_API int voss_sieve_intervals(voss_ctx* c, const uint64_t* lo, const uint64_
     if (hi[i] > c->max_hi) return fail(VOSS_ERR_RANGE, "interval %u exceeds the context limit", i);
   }
   if (n == 0) return VOSS_OK;
-  RunPlan P;
-  int rc = plan_intervals(c, lo, hi, n, 0, &P);
-  if (rc) return rc;
-  SieveArgs a;
-  rc = launch_plan(c, P, false, 0, false, c->stream, 0, &a);
-  if (rc) return rc;
-  if ((rc = c->ws.istats.ensure(sizeof(voss_interval_stats) * n))) return rc;
-  if (launch_interval_finalize(a, c->ws.out.as<IntervalOut>(), c->ws.istats.as<voss_interval_stats>(), c->stream))
-    return fail(VOSS_ERR_CUDA, "interval finalize launch failed");
-  CUDA_TRY(cudaEventRecord(c->ev2, c->stream));  // the finalize kernel counts in the launch's time
-  c->last_kernels += 1;
+  Workspace& W = c->ws;
+  cudaStream_t s = c->stream;
+  int rc;
+  IntervalRoute R;
+  route_intervals(c, lo, hi, n, 1ull << 32, &R);
+  LaunchEvents E;
+  E.ev0 = c->ev0;
+  E.evp = c->evp;
+  E.ev1 = c->ev1;
+  E.ev2 = c->ev2;
+  uint32_t kernels = 0;
+  if ((rc = W.istats.ensure(sizeof(voss_interval_stats) * n))) return rc;
+  if ((rc = launch_routed(c, W, E, R, n, s, &kernels))) return rc;
+  c->last_kernels = kernels;
   uint32_t ctr[kCtrWords];
-  CUDA_TRY(cudaMemcpyAsync(ctr, c->ws.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, c->stream));
-  CUDA_TRY(cudaMemcpyAsync(out, c->ws.istats.p, sizeof(voss_interval_stats) * n, cudaMemcpyDeviceToHost, c->stream));
-  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpyAsync(ctr, W.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(out, W.istats.p, sizeof(voss_interval_stats) * n, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
   if ((rc = check_device_error(ctr))) return rc;
   cudaEventElapsedTime(&c->sieve_ms, c->ev0, c->ev1);
   cudaEventElapsedTime(&c->total_ms, c->ev0, c->ev2);

@@ -68,6 +68,7 @@ struct Workspace {
   DevBuf pg_pa, pg_gap, pg_ok;  // gap proofs: inputs and verdicts (endpoints use mr_in / mr_out / mr_work)
   DevBuf sha_data, sha_off, sha_out;  // certificate hashing: messages, offsets, digests
   DevBuf ls_keys, ls_idx, ls_temp, ls_sorted;  // large-gap list sorted by position (large_sort.cu)
+  DevBuf sh_iv, sh_map;  // short intervals by Miller-Rabin (short_iv.cu); sieved intervals' result slots
   // Largest large-prime bitmap this workspace may use; with gbm_fixed the buffers are never
   // grown (server slots size them at creation), and launches that need more skip the pre-pass.
   size_t gbm_budget = 8ull << 30;
@@ -135,6 +136,21 @@ int plan_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, ui
 // workspace W and events E.
 int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPlan& P, bool want_large,
                    uint64_t large_cap, bool emit, cudaStream_t s, uint32_t min_gap, voss::SieveArgs* args_out);
+// A batch of intervals split between the sieve (lo, hi, map = their positions in the batch)
+// and the Miller-Rabin path for short intervals at high starts (sv, n_cand candidates).
+struct IntervalRoute {
+  std::vector<uint64_t> lo, hi;
+  std::vector<uint32_t> map;
+  std::vector<voss::ShortInterval> sv;
+  uint64_t n_cand = 0;
+};
+// Split [lo_i, hi_i) by the context's mr_route, with at most cand_cap Miller-Rabin candidates.
+void route_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, uint32_t n, uint64_t cand_cap,
+                     IntervalRoute* R);
+// Launch a routed batch of n intervals on stream s; all n results land in W.istats (lo, hi and
+// the primes 2, 3, 5 are the host's, add_small_primes).  E.ev2 is recorded after the last kernel.
+int launch_routed(voss_ctx* c, Workspace& W, const LaunchEvents& E, const IntervalRoute& R, uint32_t n,
+                  cudaStream_t s, uint32_t* kernels);
 int check_device_error(const uint32_t* ctr_host);
 std::vector<uint64_t> small_primes_in(uint64_t lo, uint64_t hi);
 // Add the primes 2, 3, 5 of [lo, hi) to a device-finalized interval result.

@@ -84,6 +84,16 @@ struct IntervalScatter {
   double vbase_d;    // vbase rounded to double (for the quotient estimate of vbase mod p)
 };
 
+// One interval of the Miller-Rabin path for short intervals (short_iv.cu).
+struct ShortInterval {
+  uint64_t base;       // 30 * floor(a / 30), a = max(lo, 7)
+  uint64_t cand_off;   // its first candidate in the launch's candidate array
+  uint32_t j0;         // wheel integers of [base, a)
+  uint32_t n_cand;     // wheel integers of [a, hi)
+  uint32_t out_index;  // position in the caller's result array
+  uint32_t pad;
+};
+
 struct TilePartial {
   uint32_t first;    // value offset (from 30 * tile byte 0) of the first prime, kNone if none
   uint32_t last;     // value offset of the last prime
@@ -158,7 +168,14 @@ int launch_reduce(const SieveArgs& a, IntervalOut* out, void* stream);
 }  // namespace voss
 struct voss_interval_stats;
 namespace voss {
-int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_interval_stats* out, void* stream);
+// out_index (nullptr: identity) gives each launch interval's position in `out`.
+int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_interval_stats* out,
+                             const uint32_t* out_index, void* stream);
+// Short intervals by Miller-Rabin (short_iv.cu): candidates into d_cand (n_cand), verdicts into
+// d_ok, the work list and its counters in d_work / d_nwork, results at d_out[out_index].
+int launch_short_intervals(const ShortInterval* d_iv, uint32_t n_iv, uint64_t n_cand, uint64_t* d_cand,
+                           uint8_t* d_ok, uint32_t* d_work, uint32_t* d_nwork, voss_interval_stats* d_out,
+                           int sm_count, void* stream);
 int launch_scatter_large(const uint32_t* primes, const uint64_t* magic, uint32_t j0, uint32_t j1,
                          const IntervalScatter* iv, uint32_t n_iv, uint32_t* gbm, int sm_count, void* stream);
 int sieve_kernel_attrs(int block, size_t smem, int* max_ctas_per_sm);

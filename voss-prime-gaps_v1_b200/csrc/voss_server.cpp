@@ -129,18 +129,17 @@ int launch_batch(voss_server* S, Slot& sl) {
       lo[i] = sl.iv[i]->lo;
       hi[i] = sl.iv[i]->hi;
     }
-    RunPlan P;
-    int rc = plan_intervals(c, lo.data(), hi.data(), sl.n_iv, 0, &P);
+    // short intervals at high starts by Miller-Rabin, within the slot's candidate buffers (the
+    // batch's own Miller-Rabin requests reuse them later on the same stream)
+    IntervalRoute R;
+    route_intervals(c, lo.data(), hi.data(), sl.n_iv, S->cfg.max_batch_candidates, &R);
+    uint32_t kernels = 0;
+    int rc = launch_routed(c, sl.ws, sl.E, R, sl.n_iv, s, &kernels);
     if (rc) return rc;
-    SieveArgs a;
-    rc = launch_plan_ws(c, sl.ws, sl.E, P, false, 0, false, s, 0, &a);
-    if (rc) return rc;
-    if (voss::launch_interval_finalize(a, sl.ws.out.as<IntervalOut>(), sl.ws.istats.as<voss_interval_stats>(), s))
-      return fail(VOSS_ERR_CUDA, "interval finalize launch failed");
     CUDA_TRY(cudaMemcpyAsync(sl.h_istats, sl.ws.istats.p, sizeof(voss_interval_stats) * sl.n_iv,
                              cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaMemcpyAsync(sl.h_ctr, sl.ws.counters.p, sizeof(uint32_t) * kCtrWords, cudaMemcpyDeviceToHost, s));
-    S->launches += 4;
+    S->launches += kernels;
   } else {
     std::memset(sl.h_ctr, 0, sizeof(uint32_t) * kCtrWords);
   }
@@ -305,6 +304,8 @@ Slot* make_slot(voss_server* S, int* rc) {
   W.gbm_budget = C.max_batch_bitmap_bytes;
   W.gbm_fixed = true;
   if (W.gbm_budget && ((e = W.gbm.ensure(W.gbm_budget)) || (e = W.scat.ensure(sizeof(voss::IntervalScatter) * nreq))))
+    return bad(e);
+  if ((e = W.sh_iv.ensure(sizeof(voss::ShortInterval) * nreq)) || (e = W.sh_map.ensure(sizeof(uint32_t) * nreq)))
     return bad(e);
   if (cudaMallocHost(&sl->h_istats, sizeof(voss_interval_stats) * nreq) != cudaSuccess ||
       cudaMallocHost(&sl->h_mr_in, 8 * (C.max_batch_candidates + 1)) != cudaSuccess ||

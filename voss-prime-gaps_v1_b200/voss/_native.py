@@ -63,7 +63,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [
         ("block_threads", c_uint32), ("chunk_words", c_uint32), ("ctas_per_sm", c_uint32),
         ("coop_div", c_uint32), ("mult_factor", c_uint32), ("medium_mode", c_uint32),
-        ("walk_sixteenths", c_uint32), ("reserved", c_uint32 * 1),
+        ("walk_sixteenths", c_uint32), ("mr_route", c_uint32),
     ]
 
 

@@ -112,7 +112,7 @@ class Context:
         t = N.Tuning()
         N.check(self.lib.voss_ctx_get_tuning(self._h, byref(t)))
         return {k: getattr(t, k) for k in ("block_threads", "chunk_words", "ctas_per_sm", "coop_div", "mult_factor",
-                                           "medium_mode", "walk_sixteenths")}
+                                           "medium_mode", "walk_sixteenths", "mr_route")}
 
     def set_tuning(self, **kw) -> dict:
         t = N.Tuning()

@@ -91,6 +91,64 @@ def test_bench_sieve_work_equals_oracle():
         assert bench.sieve_work(n) == O.sieve_work(n), n
 
 
+def _bench():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    return bench
+
+
+def test_bench_interval_work_terms():
+    """The interval roofline's work terms: the offsets are exact (one per interval and base
+    prime <= isqrt(hi - 1)); the expected clear counts agree with a direct count of the wheel
+    multiples of each prime (>= p^2) within a few per cent on intervals of 10^6."""
+    bench = _bench()
+    lo = np.array([10**8, 10**10, 3 * 10**11], dtype=np.uint64)
+    hi = lo + np.array([10**6, 10**6, 10**6], dtype=np.uint64)
+    p_large = 20_000
+    w = bench.interval_work(lo, hi, p_large)
+    P = bench.primes_upto(math.isqrt(int(hi.max()) - 1)).astype(np.int64)
+    assert w["first_hit_offsets"] == sum(int((P <= math.isqrt(int(h) - 1)).sum()) for h in hi)
+    exact = [0, 0, 0]
+    cuts = [7, 37, p_large, 1 << 62]
+    for a, b in zip(lo.tolist(), hi.tolist()):
+        for p in P[P <= math.isqrt(b - 1)].tolist():
+            m0 = max(-(-a // p), p)            # first multiple >= max(a, p^2), as a multiplier
+            m1 = (b - 1) // p
+            if m1 < m0:
+                continue
+            def coprime_upto(x):               # multipliers m <= x coprime to 30
+                return 8 * (x // 30) + sum(1 for r in range(1, x % 30 + 1) if math.gcd(r, 30) == 1)
+            c = coprime_upto(m1) - coprime_upto(m0 - 1)
+            exact[next(i for i in range(3) if cuts[i] <= p < cuts[i + 1])] += c
+    got = [w["presieve_primes_hits"], w["tile_hits"], w["prepass_hits"]]
+    for g, e in zip(got, exact):
+        assert abs(g - e) <= 0.03 * e + 50, (got, exact)
+
+
+def test_bench_mr_products_small_cases():
+    """The Miller-Rabin roofline's product count for single candidates, by hand."""
+    bench = _bench()
+    assert bench.mr_mulmods(np.array([2, 3, 4, 9, 35, 37], dtype=np.uint64)) == (0, 0)  # trial division
+    # 41: d = 5 (3 bits, 2 set), r = 3; base 2: 3 squarings, 2^5 = 32 = -9, squarings to -1:
+    # 32^2 = 40 = -1 after one step.  Bases 3, 5, 7, 11, 13: 3 + 2 products each plus the steps.
+    n = 41
+    want = 0
+    for a in (2, 3, 5, 7, 11, 13):
+        want += 3 + (0 if a == 2 else 2)
+        x = pow(a, 5, n)
+        j = 0
+        while x not in (1, n - 1) and j < 2:
+            x = x * x % n
+            j += 1
+        want += j
+    assert bench.mr_mulmods(np.array([n], dtype=np.uint64)) == (want, 0)
+    big = (1 << 63) + 29                       # above 2^63: counted as a full-width modulus
+    s, f = bench.mr_mulmods(np.array([big], dtype=np.uint64))
+    assert s == 0 and f > 0
+
+
 @pytest.mark.parametrize("lo,hi,compat,seg", [
     (1, 20000, True, 30), (1, 20000, True, 330), (1, 50000, True, 30_000_000_000),
     (1, 20000, False, 0), (2, 3, False, 0), (0, 8, False, 0), (9000, 31000, False, 0),

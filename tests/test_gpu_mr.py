@@ -99,3 +99,19 @@ def test_prove_gaps_long_joined_and_high(gpu_ctx):
     np.testing.assert_array_equal(got[:nb + nj], checker(P[:nb + nj], G[:nb + nj]))
     assert got[:nb].all() and not got[nb:nb + nj].any()
     assert got[nb + nj:-1].all() and not got[-1]
+
+
+def test_mr_large_host_batches_through_staging(gpu_ctx):
+    """Batches of 2^20 candidates or more cross through the context's pinned staging buffers
+    (one and several 2^24-candidate chunks, odd sizes); their verdicts equal those of small
+    batches, which are copied straight from the caller's memory, and the reference verifier's."""
+    rng = np.random.default_rng(5)
+    for size in (3 * 2**20 + 7, 2**24 + 12345):
+        n = rng.integers(0, 2**63, size=size, dtype=np.uint64) * 2 + 1
+        n[::97] = rng.integers(0, 2**40, size=n[::97].size, dtype=np.uint64)  # even and small values too
+        got = gpu_ctx.mr_verify(n)
+        step = (1 << 20) - 1
+        small = np.concatenate([gpu_ctx.mr_verify(n[i:i + step]) for i in range(0, size, step)])
+        np.testing.assert_array_equal(got, small)
+        sel = np.arange(0, size, 53)
+        np.testing.assert_array_equal(got[sel], checker(n[sel]))

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "voss.h"
@@ -321,6 +322,45 @@ int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_c
   E.ev1 = c->ev1;
   E.ev2 = c->ev2;
   return launch_plan_ws(c, c->ws, E, P, want_large, large_cap, emit, s, min_gap, args_out);
+}
+
+// memcpy split over host threads: one thread copies from pageable memory at a fraction of the
+// host's memory bandwidth.
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+  const size_t kMinPart = 8u << 20;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t parts = std::min<size_t>({(size_t)std::min(hw, 8u), bytes / kMinPart + 1});
+  if (parts <= 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t step = (bytes / parts + 63) & ~(size_t)63;
+  std::vector<std::thread> th;
+  for (size_t i = 1; i < parts; ++i) {
+    const size_t a = std::min(bytes, i * step), b = std::min(bytes, (i + 1) * step);
+    if (a < b)
+      th.emplace_back([=] { std::memcpy((char*)dst + a, (const char*)src + a, b - a); });
+  }
+  std::memcpy(dst, src, std::min(bytes, step));
+  for (auto& t : th) t.join();
+}
+
+// The context's two pinned staging buffers, at least `entries` 64-bit words each (grow-only).
+int ensure_stage(voss_ctx* c, size_t entries) {
+  if (entries <= c->h_stage_cap) return VOSS_OK;
+  for (int b = 0; b < 2; ++b) {
+    CUDA_TRY(cudaEventSynchronize(c->ev_stage[b]));
+    if (c->h_stage[b]) cudaFreeHost(c->h_stage[b]);
+    c->h_stage[b] = nullptr;
+  }
+  c->h_stage_cap = 0;
+  for (int b = 0; b < 2; ++b)
+    if (cudaMallocHost(&c->h_stage[b], entries * sizeof(uint64_t)) != cudaSuccess) {
+      c->h_stage[b] = nullptr;
+      return fail(VOSS_ERR_NOMEM, "cudaMallocHost of the staging buffers failed");
+    }
+  c->h_stage_cap = entries;
+  return VOSS_OK;
 }
 
 // Route a batch of intervals (see voss_host.h) and launch it.
@@ -708,6 +748,8 @@ VOSS_API int voss_ctx_create(int device, uint64_t max_hi, voss_ctx** out) {
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_copy, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_stage[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_stage[1], cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->evp) != cudaSuccess)
     return bail(fail(VOSS_ERR_CUDA, "stream/event creation failed"));
@@ -746,6 +788,10 @@ VOSS_API void voss_ctx_destroy(voss_ctx* c) {
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->ev_copy) cudaEventDestroy(c->ev_copy);
   if (c->h_large) cudaFreeHost(c->h_large);
+  for (int b = 0; b < 2; ++b) {
+    if (c->h_stage[b]) cudaFreeHost(c->h_stage[b]);
+    if (c->ev_stage[b]) cudaEventDestroy(c->ev_stage[b]);
+  }
   delete c;
 }
 
@@ -980,26 +1026,61 @@ VOSS_API int voss_mr_verify(voss_ctx* c, const uint64_t* n, uint64_t count, uint
   Workspace& W = c->ws;
   int rc;
   // context-owned, grow-only buffers: repeated calls do not allocate.  The candidates cross in
-  // chunks on the copy stream while the previous chunk is tested on `stream` (a copy from
-  // pageable memory returns once staged, without waiting for the device); the verdicts come
-  // back in one copy at the end (a device-to-host copy into pageable memory would block).
+  // chunks on the copy stream while the previous chunk is tested on `stream`.  Large batches go
+  // through two pinned staging buffers that host threads fill (chunk i + 1 is copied in while
+  // chunk i crosses and chunk i - 1 is tested), and the verdicts come back the same way; small
+  // ones are copied straight from the caller's memory.
   constexpr uint64_t kChunk = 1ull << 24;
   const uint64_t per = std::min(count, kChunk);
+  const bool staged = count >= (1ull << 20);
   if ((rc = W.mr_in.ensure(count * 8)) || (rc = W.mr_out.ensure(count)) ||
       (rc = W.mr_work.ensure(sizeof(uint32_t) * (per + 8))))
     return rc;
+  if (staged && (rc = ensure_stage(c, per))) return rc;
   uint64_t* d_in = W.mr_in.as<uint64_t>();
   uint8_t* d_out = W.mr_out.as<uint8_t>();
   uint32_t* work = W.mr_work.as<uint32_t>();
-  for (uint64_t off = 0; off < count; off += kChunk) {
+  uint64_t i = 0;
+  for (uint64_t off = 0; off < count; off += kChunk, ++i) {
     const uint64_t k = std::min(kChunk, count - off);
-    CUDA_TRY(cudaMemcpyAsync(d_in + off, n + off, k * 8, cudaMemcpyHostToDevice, c->copy_stream));
+    if (staged) {
+      const int b = (int)(i & 1);
+      CUDA_TRY(cudaEventSynchronize(c->ev_stage[b]));  // buffer b's previous transfer is done
+      parallel_copy(c->h_stage[b], n + off, k * 8);
+      CUDA_TRY(cudaMemcpyAsync(d_in + off, c->h_stage[b], k * 8, cudaMemcpyHostToDevice, c->copy_stream));
+      CUDA_TRY(cudaEventRecord(c->ev_stage[b], c->copy_stream));
+    } else {
+      CUDA_TRY(cudaMemcpyAsync(d_in + off, n + off, k * 8, cudaMemcpyHostToDevice, c->copy_stream));
+    }
     CUDA_TRY(cudaEventRecord(c->ev_copy, c->copy_stream));
     CUDA_TRY(cudaStreamWaitEvent(s, c->ev_copy, 0));
     if (launch_mr(d_in + off, k, d_out + off, work + 8, work, s, c->sm_count))
       return fail(VOSS_ERR_CUDA, "Miller-Rabin launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
-  CUDA_TRY(cudaMemcpyAsync(is_prime, d_out, count, cudaMemcpyDeviceToHost, s));
+  if (!staged) {
+    CUDA_TRY(cudaMemcpyAsync(is_prime, d_out, count, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return VOSS_OK;
+  }
+  // verdicts: chunk j crosses into buffer j & 1 while chunk j - 1 is copied out by host threads
+  // (the input transfers are complete: every launch on `stream` waited for them)
+  const uint64_t ob = c->h_stage_cap * sizeof(uint64_t);
+  uint64_t prev_off = 0, prev_k = 0;
+  uint64_t j = 0;
+  for (uint64_t off = 0; off < count; off += ob, ++j) {
+    const uint64_t k = std::min(ob, count - off);
+    const int b = (int)(j & 1);
+    CUDA_TRY(cudaMemcpyAsync(c->h_stage[b], d_out + off, k, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaEventRecord(c->ev_stage[b], s));
+    if (j > 0) {
+      CUDA_TRY(cudaEventSynchronize(c->ev_stage[b ^ 1]));
+      parallel_copy(is_prime + prev_off, c->h_stage[b ^ 1], prev_k);
+    }
+    prev_off = off;
+    prev_k = k;
+  }
+  CUDA_TRY(cudaEventSynchronize(c->ev_stage[(j - 1) & 1]));
+  parallel_copy(is_prime + prev_off, c->h_stage[(j - 1) & 1], prev_k);
   CUDA_TRY(cudaStreamSynchronize(s));
   return VOSS_OK;
 }

@@ -125,6 +125,12 @@ struct voss_ctx {
   // the list (sorted on the device), so that repeated calls touch no fresh pages
   voss_large_gap* h_large = nullptr;
   size_t h_large_cap = 0;
+  // pinned staging of large host batches (Miller-Rabin candidates in, verdicts out): two
+  // buffers, one filled by host threads while the other crosses; ev_stage[b] marks the end of
+  // buffer b's last transfer
+  uint64_t* h_stage[2] = {nullptr, nullptr};
+  size_t h_stage_cap = 0;  // 64-bit entries per buffer
+  cudaEvent_t ev_stage[2] = {nullptr, nullptr};
 };
 
 namespace voss_host {

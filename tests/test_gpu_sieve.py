@@ -222,3 +222,17 @@ def test_short_intervals_by_miller_rabin_equal_the_sieve(gpu_ctx_big):
         gpu_ctx_big.set_tuning(**t0)
     sel = np.nonzero(hi < 10**16)[0][:16]
     _same_intervals(routed[sel], O.sieve_intervals(lo[sel], hi[sel]))
+
+
+def test_large_interval_batches_through_staging(gpu_ctx):
+    """Batches whose results exceed 8 MB (over 1023 intervals) come back through the context's
+    pinned staging; they equal the same intervals in small batches and the oracle."""
+    rng = np.random.default_rng(23)
+    k = 2500
+    lo = (10 ** rng.uniform(1, 12.5, k)).astype(np.uint64)
+    hi = lo + (10 ** rng.uniform(0, 4, k)).astype(np.uint64)
+    big = gpu_ctx.sieve_intervals(lo, hi)
+    small = np.concatenate([gpu_ctx.sieve_intervals(lo[i:i + 500], hi[i:i + 500]) for i in range(0, k, 500)])
+    _same_intervals(big, small)
+    sel = np.arange(0, k, 37)
+    _same_intervals(big[sel], O.sieve_intervals(lo[sel], hi[sel]))

@@ -913,8 +913,17 @@ VOSS_API int voss_sieve_intervals(voss_ctx* c, const uint64_t* lo, const uint64_
   c->last_kernels = kernels;
   uint32_t ctr[kCtrWords];
   CUDA_TRY(cudaMemcpyAsync(ctr, W.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(out, W.istats.p, sizeof(voss_interval_stats) * n, cudaMemcpyDeviceToHost, s));
+  // large results (8 KB per interval) come back through pinned staging, copied out by host threads
+  const size_t res_bytes = sizeof(voss_interval_stats) * n;
+  const bool staged = res_bytes >= (8u << 20);
+  if (staged) {
+    if ((rc = ensure_stage(c, res_bytes / sizeof(uint64_t) + 1))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(c->h_stage[0], W.istats.p, res_bytes, cudaMemcpyDeviceToHost, s));
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(out, W.istats.p, res_bytes, cudaMemcpyDeviceToHost, s));
+  }
   CUDA_TRY(cudaStreamSynchronize(s));
+  if (staged) parallel_copy(out, c->h_stage[0], res_bytes);
   if ((rc = check_device_error(ctr))) return rc;
   cudaEventElapsedTime(&c->sieve_ms, c->ev0, c->ev1);
   cudaEventElapsedTime(&c->total_ms, c->ev0, c->ev2);

@@ -115,3 +115,22 @@ def test_mr_large_host_batches_through_staging(gpu_ctx):
         np.testing.assert_array_equal(got, small)
         sel = np.arange(0, size, 53)
         np.testing.assert_array_equal(got[sel], checker(n[sel]))
+
+
+def test_prove_gaps_large_batches_through_staging(gpu_ctx):
+    """2^20 gaps or more cross through the pinned staging buffers; the verdicts (true gaps and
+    altered ones) equal those of small batches and of the reference verifier on a sample."""
+    gaps = gpu_ctx.gaps_at_least(1, 5 * 10**9, 100)
+    assert gaps.size > (1 << 20)
+    p = gaps["position"].astype(np.uint64)
+    g = gaps["gap"].astype(np.int32)
+    g[::11] += 2                                   # a larger gap whose interior holds a prime
+    got = gpu_ctx.prove_gaps(p, g)
+    step = (1 << 20) - 1
+    small = np.concatenate([gpu_ctx.prove_gaps(p[i:i + step], g[i:i + step]) for i in range(0, p.size, step)])
+    np.testing.assert_array_equal(got, small)
+    assert got[1::11].all() and not got[::11].any()
+    import os
+    sel = np.arange(0, p.size, 997)
+    ref = O.ref_prove_gaps(p[sel], g[sel]) if os.path.exists(O.REF_VERIFY_SO) else O.prove_gaps(p[sel], g[sel])
+    np.testing.assert_array_equal(got[sel], ref)

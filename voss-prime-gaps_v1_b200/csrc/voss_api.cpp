@@ -1109,14 +1109,22 @@ VOSS_API int voss_prove_gaps(voss_ctx* c, const uint64_t* p_after, const int32_t
       (rc = W.mr_in.ensure(2 * count * 8)) || (rc = W.mr_out.ensure(2 * count)) ||
       (rc = W.mr_work.ensure(sizeof(uint32_t) * (2 * count + 8))))
     return rc;
-  CUDA_TRY(cudaMemcpyAsync(W.pg_pa.p, p_after, count * 8, cudaMemcpyHostToDevice, s));
-  CUDA_TRY(cudaMemcpyAsync(W.pg_gap.p, gap, count * 4, cudaMemcpyHostToDevice, s));
+  // large batches cross through the pinned staging buffers (filled and emptied by host threads)
+  const bool staged = count >= (1ull << 20);
+  if (staged) {
+    if ((rc = ensure_stage(c, count))) return rc;
+    parallel_copy(c->h_stage[0], p_after, count * 8);
+    parallel_copy(c->h_stage[1], gap, count * 4);
+  }
+  CUDA_TRY(cudaMemcpyAsync(W.pg_pa.p, staged ? (const void*)c->h_stage[0] : p_after, count * 8, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(W.pg_gap.p, staged ? (const void*)c->h_stage[1] : gap, count * 4, cudaMemcpyHostToDevice, s));
   uint32_t* work = W.mr_work.as<uint32_t>();
   if (launch_prove_gaps(W.pg_pa.as<uint64_t>(), W.pg_gap.as<int32_t>(), count, W.pg_ok.as<uint8_t>(),
                         W.mr_in.as<uint64_t>(), W.mr_out.as<uint8_t>(), work + 8, work, s, c->sm_count))
     return fail(VOSS_ERR_CUDA, "gap proof launch failed");
-  CUDA_TRY(cudaMemcpyAsync(ok, W.pg_ok.p, count, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(staged ? (void*)c->h_stage[0] : ok, W.pg_ok.p, count, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
+  if (staged) parallel_copy(ok, c->h_stage[0], count);
   return VOSS_OK;
 }
 

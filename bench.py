@@ -20,6 +20,21 @@ range/s = integers sieved per second (higher is better).
   ref_cuda   the reference's voss_v7_live.cu rebuilt for sm_100a (oracle/_ref), its printed
              TOTAL TIME at the same N (rank 0, N = 1), when the binary is present.
 
+  roofline_split  the tile kernel's time split into its sieve and extraction phases (phase
+             shares from the phase-timing build, run in a child process), each against the
+             same shared-memory peak.
+
+At 1 GPU the line also carries the other halves of the metric, each a complete sub-line with
+its own value, e2e, roofline, clocks and baseline (same --steps / --warmup):
+  intervals  4096 seeded intervals (a log-uniform [1e10, 1e16], L log-uniform [1e4, 1e8]) in
+             one batched persistent launch versus one plain launch per interval;
+  mr         10^8 Miller-Rabin candidates (5e7 primes below 1e12 + 5e7 random odd u64) and the
+             interior proofs of all gaps >= 200 below 1e12, beside the reference verifier;
+  serve      seeded Poisson request streams at 1e2, 1e3, 1e4 req/s through the
+             continuous-batching server (p50/p99) versus plain launches, and the capacity of
+             both with every request offered at once (capacity_ratio_vs_plain).
+`--workload intervals|mr|serve` prints one of them alone; `--sub ""` leaves them out.
+
 Multi-GPU (torchrun): weak scaling; rank r sieves [r*N + 1, (r+1)*N], the statistics are
 all-gathered over NCCL and merged (voss_stats_merge) into those of [1, world*N].
 
@@ -69,6 +84,13 @@ def parse():
     ap.add_argument("--plain-seconds", type=float, default=20.0, help="serving: cap on the plain-launch replay")
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="intervals: skip the one-launch-per-interval comparison")
+    ap.add_argument("--capacity-requests", type=int, default=10000,
+                    help="serving: requests offered at once for the capacity comparison")
+    ap.add_argument("--sub", default="intervals,mr,serve",
+                    help="range workload at 1 GPU: the other workloads to run after it and attach to its line "
+                         "(comma list of intervals, mr, serve; empty for none)")
+    ap.add_argument("--no-extract-split", action="store_true")
+    ap.add_argument("--phase-probe", action="store_true", help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -352,7 +374,7 @@ def interval_batch(k: int, seed: int = 20261203):
     return a, a + ln
 
 
-def run_intervals(a) -> None:
+def run_intervals(a) -> dict:
     """Batched uneven intervals: one persistent launch over the (interval, tile) work queue
     versus one plain launch per interval; results must agree bit for bit."""
     import numpy as np
@@ -429,7 +451,8 @@ def run_intervals(a) -> None:
                                             "total_wall_s": plain_wall}
         out["speedup_vs_plain"] = {"device": plain_dev / (bd * 1e3), "e2e": plain_wall / bw}
         out["bit_exact_vs_plain"] = bool(same)
-    print(json.dumps(out), flush=True)
+    del ctx
+    return out
 
 
 def mr_candidates(ctx, half: int, seed: int = 20261203):
@@ -445,7 +468,7 @@ def mr_candidates(ctx, half: int, seed: int = 20261203):
     return n[perm], perm < p.size
 
 
-def run_mr(a) -> None:
+def run_mr(a) -> dict:
     """Batched verification: 1e8 candidates through deterministic Miller-Rabin (12 bases), and
     the interior-composite proof of every gap >= 200 below 1e12."""
     import numpy as np
@@ -547,14 +570,17 @@ def run_mr(a) -> None:
         "clocks": clk,
         "gpu_launches": 2 * a.steps,
     }
-    print(json.dumps(out), flush=True)
+    del ctx
+    return out
 
 
-def run_serve(a) -> None:
+def run_serve(a) -> dict:
     """Serving: seeded Poisson streams of mixed requests (70% interval sieve + gap statistics,
     start log-uniform [1e9, 1e18], length log-uniform [1e3, 1e9]; 30% Miller-Rabin batches of
     10^U(3,6) odd u64) through the continuous-batching server, versus the same stream served with
-    one plain launch per request."""
+    one plain launch per request.  Then the capacity of both: the same kind of requests all
+    offered at once (arrival times zero), served by the server and one at a time by plain
+    launches; capacity_ratio_vs_plain = served req/s / plain req/s."""
     import numpy as np
     import voss
     from voss.serve import Server, request_stream, serve_plain, serve_stream
@@ -566,9 +592,12 @@ def run_serve(a) -> None:
     for rate in [float(x) for x in a.rates.split(",")]:
         count = int(min(30000, max(50, rate * a.serve_seconds)))
         stream = request_stream(rate, count, seed=20261203)
+        clocks = ClockSampler(0)
+        clocks.start()
         with Server(ctx) as srv:
             lat, wall, _, err = serve_stream(srv, stream)
             st = srv.stats()
+        clk = clocks.stop()
         done = lat[~np.isnan(lat)]
         # the same stream served one request at a time with plain launches, in arrival order,
         # until the time cap (latency from arrival, so it includes queueing behind earlier ones)
@@ -579,12 +608,34 @@ def run_serve(a) -> None:
             "p50_ms": float(np.percentile(done, 50) * 1e3), "p99_ms": float(np.percentile(done, 99) * 1e3),
             "mean_ms": float(done.mean() * 1e3), "throughput_req_s": count / wall,
             "batches": st["batches"], "mean_batch_requests": st["mean_batch_requests"],
-            "max_inflight_batches": st["max_inflight_batches"],
+            "max_inflight_batches": st["max_inflight_batches"], "clocks": clk,
             "plain": {"requests_served": plain_n, "p50_ms": float(np.percentile(pl, 50) * 1e3),
                       "p99_ms": float(np.percentile(pl, 99) * 1e3), "throughput_req_s": plain_n / plain_wall,
                       "note": "one request at a time in arrival order (time-capped replay of the same stream); "
                               "latency from arrival includes the wait behind earlier requests"},
         })
+        del stream
+    # capacity: every request offered at time zero (request_stream draws the arrival gaps first,
+    # so these payloads are those of the 1e4 req/s stream of the same length and seed)
+    cap_n = a.capacity_requests
+    burst = request_stream(1e12, cap_n, seed=20261203)
+    clocks = ClockSampler(0)
+    clocks.start()
+    with Server(ctx) as srv:
+        lat, wall, _, err = serve_stream(srv, burst)
+        st = srv.stats()
+    clk = clocks.stop()
+    done = lat[~np.isnan(lat)]
+    pl, plain_wall = serve_plain(ctx, burst, time_cap=a.plain_seconds)
+    served_rps, plain_rps = cap_n / wall, len(pl) / plain_wall
+    capacity = {"requests": cap_n, "errors": len(err), "served_req_s": served_rps, "served_wall_s": wall,
+                "served_p50_ms": float(np.percentile(done, 50) * 1e3),
+                "served_p99_ms": float(np.percentile(done, 99) * 1e3),
+                "batches": st["batches"], "mean_batch_requests": st["mean_batch_requests"],
+                "plain_req_s": plain_rps, "plain_requests_served": len(pl), "plain_wall_s": plain_wall,
+                "clocks": clk,
+                "note": "all requests offered at once; served = continuous batching over 4 slots, plain = one "
+                        "launch per request in order (time-capped)"}
     top = rows[-1]
     out = {
         "metric": "serving: completed requests/s with p50/p99 latency (continuous batching)",
@@ -593,23 +644,63 @@ def run_serve(a) -> None:
         "data": "synthetic: seeded Poisson arrivals (PCG64 seed 20261203)",
         "config": {"workload": "mixed interval + Miller-Rabin requests", "slots": 4, "base_primes_to": "1e9"},
         "rates": rows,
+        "capacity": capacity,
+        "capacity_ratio_vs_plain": served_rps / plain_rps,
     }
-    print(json.dumps(out), flush=True)
+    del ctx
+    return out
+
+
+def extract_split(n: int) -> dict | None:
+    """Share of the tile kernel's time in each phase, from the phase-timing build
+    (libvoss_timing.so: a block barrier and a clock64 stamp at every phase boundary), run in a
+    child process so that it does not replace the product library in this one."""
+    lib = os.path.join(ROOT, "voss-prime-gaps_v1_b200", "voss", "_lib", "libvoss_timing.so")
+    if not os.path.exists(lib):
+        return None
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--phase-probe", "--n", str(n)],
+                       capture_output=True, text=True, timeout=600)
+    try:
+        return json.loads(r.stdout.strip().splitlines()[-1])
+    except (ValueError, IndexError):
+        return {"unavailable": f"phase probe rc={r.returncode}: {r.stderr.strip()[-200:]}"}
+
+
+PHASES = ("claim_flush", "header", "fill", "small_primes", "medium_primes", "large_primes", "restore",
+          "extract_scan", "extract_walk", "extract_reduce")
+
+
+def run_phase_probe(n: int) -> None:
+    """Child process of extract_split: one REF_COMPAT sieve of [1, n] through the timing build."""
+    import ctypes
+    import voss
+    from voss import _native as N
+    lib = os.path.join(ROOT, "voss-prime-gaps_v1_b200", "voss", "_lib", "libvoss_timing.so")
+    ctx = voss.Context(n + 1, lib_path=lib)
+    L = ctx.lib
+    L.voss_debug_phase_cycles.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int, ctypes.c_int]
+    ctx.sieve_range(1, 10**9 + 1, compat=True, seg_num=SEG_NUM)  # warm-up
+    buf = (ctypes.c_ulonglong * 10)()
+    N.check(L.voss_debug_phase_cycles(buf, 10, 1))
+    ctx.sieve_range(1, n + 1, compat=True, seg_num=SEG_NUM)
+    N.check(L.voss_debug_phase_cycles(buf, 10, 1))
+    cyc = [int(x) for x in buf]
+    tot = float(sum(cyc)) or 1.0
+    print(json.dumps({"cycles": dict(zip(PHASES, cyc)), "share": {k: c / tot for k, c in zip(PHASES, cyc)},
+                      "timing_build_ms": ctx.last_kernel_ms()[1]}), flush=True)
 
 
 def main():
     a = parse()
+    if a.phase_probe:
+        run_phase_probe(a.n)
+        return
     if a.impl == "reference":
         run_reference_arm(a)
         return
-    if a.workload == "intervals":
-        run_intervals(a)
-        return
-    if a.workload == "mr":
-        run_mr(a)
-        return
-    if a.workload == "serve":
-        run_serve(a)
+    if a.workload in ("intervals", "mr", "serve"):
+        fn = {"intervals": run_intervals, "mr": run_mr, "serve": run_serve}[a.workload]
+        print(json.dumps(fn(a)), flush=True)
         return
     import numpy as np
     import torch
@@ -733,12 +824,44 @@ def main():
                    "large_gaps": r.large_total if r else None},
     }
     if world == 1:
+        if not a.no_extract_split:
+            sp = extract_split(n)
+            if sp and "share" in sp:
+                sh = sp["share"]
+                ext = sh["extract_scan"] + sh["extract_walk"] + sh["extract_reduce"]
+                sie = sh["fill"] + sh["small_primes"] + sh["medium_primes"] + sh["large_primes"] + sh["restore"]
+                # extraction: one 32-bit read of every bitmap word (N/30 B) + three 32-bit shared-memory
+                # RMWs per prime (gap bin and two residue-class counters, 8 B each)
+                ext_bytes = (hi - lo) / 30.0 + 24.0 * r.prime_count
+                ext_ms, sie_ms = ext * kernel_ms, sie * kernel_ms
+                out["roofline_split"] = {
+                    "source": "phase shares of the tile kernel from the phase-timing build (libvoss_timing.so, "
+                              "clock64 stamps summed over CTAs) applied to this run's kernel_ms",
+                    "phase_share": sh,
+                    "sieve": {"ms": sie_ms, "algorithmic_bytes": 8.0 * h,
+                              "achieved": 8.0 * h / (sie_ms * 1e-3) / 1e9, "peak": smem_peak, "unit": "GB/s",
+                              "frac": 8.0 * h / (sie_ms * 1e-3) / 1e9 / smem_peak,
+                              "phases": "fill, small/medium/large primes, restore"},
+                    "extract": {"ms": ext_ms, "algorithmic_bytes": ext_bytes,
+                                "achieved": ext_bytes / (ext_ms * 1e-3) / 1e9, "peak": smem_peak, "unit": "GB/s",
+                                "frac": ext_bytes / (ext_ms * 1e-3) / 1e9 / smem_peak,
+                                "bytes_note": "N/30 B of bitmap reads + 24 B (three 32-bit RMWs) per prime",
+                                "phases": "last-prime scan, in-order walk with counters, tile reduce"},
+                }
+            elif sp:
+                out["roofline_split"] = sp
         if not a.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(n, a.cpu_seconds)
         if not a.no_ref_cuda:
             rc = ref_cuda_baseline(n)
             if rc is not None:
                 out["ref_cuda"] = rc
+        del ctx
+        subs = {"intervals": run_intervals, "mr": run_mr, "serve": run_serve}
+        for name in [x for x in a.sub.split(",") if x]:
+            out[name] = subs[name](a)
+        print(json.dumps(out), flush=True)
+        return
     print(json.dumps(out), flush=True)
     del ctx
     if dist is not None:

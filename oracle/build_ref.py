@@ -10,7 +10,7 @@ does the same substitution in memory, writes the patched text to a temporary dir
 the repository, and compiles it for sm_100a with the reference's own flags (-O3,
 src/voss_master.py:138-140).  The reference source is read from its tree and never copied here.
 
-usage: python oracle/build_ref.py [--ref /root/reference] [--n 1000000000 ...]
+usage: python oracle/build_ref.py [--ref REFERENCE_CHECKOUT] [--n 1000000000 ...]   (--ref defaults to $VOSS_REF)
 """
 import argparse
 import math
@@ -76,7 +76,7 @@ def build(ref: str, ns, mem_gb: float = 180.0, force: bool = False) -> list:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("VOSS_REF"), required=not os.environ.get("VOSS_REF"))
     ap.add_argument("--n", type=int, nargs="*", default=DEFAULT_NS)
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()

@@ -274,7 +274,20 @@ static inline void o_prime(o_acc* a, uint64_t p) {
 /* Sieve [lo, hi) (window by window) feeding primes into `a` in ascending order.
  * bp: all primes up to at least isqrt(hi - 1), including 2. */
 static void o_sieve_span(o_acc* a, uint64_t lo, uint64_t hi, const uint32_t* bp, uint64_t nbp) {
-  const uint64_t WIN = 1u << 20; /* odd slots per window */
+  /* Odd slots per window: every window costs one division per base prime up to its isqrt,
+   * so windows grow with that count (2^20 .. 2^24 slots) to keep the divisions a small part
+   * of the marking at starts near 10^16 .. 10^18 (5.8e6 .. 5.1e7 base primes). */
+  uint64_t WIN = 1u << 20;
+  {
+    uint64_t r = hi > 1 ? o_isqrt(hi - 1) : 1, used = 0;
+    uint64_t lo_k = 0, hi_k = nbp; /* number of base primes <= r (bp is ascending) */
+    while (lo_k < hi_k) {
+      uint64_t mid = (lo_k + hi_k) / 2;
+      if (bp[mid] <= r) lo_k = mid + 1; else hi_k = mid;
+    }
+    used = lo_k;
+    while (WIN < used && WIN < (1u << 24)) WIN <<= 1;
+  }
   if (lo < 2) lo = 2;
   if (lo >= hi) return;
   if (lo <= 2 && 2 < hi) o_prime(a, 2);
@@ -384,7 +397,11 @@ int oracle_sieve_range(uint64_t lo, uint64_t hi, uint32_t flags, uint64_t seg_nu
   return VOSS_OK;
 }
 
-/* Per-interval statistics with the semantics of voss_sieve_intervals. */
+/* Per-interval statistics with the semantics of voss_sieve_intervals.  Each interval is cut
+ * into chunks of at most O_IV_CHUNK integers; the chunks of all intervals run in parallel
+ * and are merged per interval in order (o_merge adds the gap across each seam), so one
+ * interval of 10^8 integers is not left to a single thread. */
+#define O_IV_CHUNK ((uint64_t)1 << 24)
 int oracle_sieve_intervals(const uint64_t* lo, const uint64_t* hi, uint32_t n, int threads,
                            voss_interval_stats* out) {
   uint64_t maxhi = 2;
@@ -394,27 +411,49 @@ int oracle_sieve_intervals(const uint64_t* lo, const uint64_t* hi, uint32_t n, i
   }
   uint64_t nbp = 0;
   uint32_t* bp = oracle_base_primes(o_isqrt(maxhi - 1) + 1, &nbp);
+  /* chunk c of interval i covers [lo_i + c*O_IV_CHUNK, min(hi_i, lo_i + (c+1)*O_IV_CHUNK)) */
+  uint64_t* first_chunk = (uint64_t*)malloc(((size_t)n + 1) * sizeof(uint64_t));
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    first_chunk[i] = total;
+    uint64_t len = hi[i] - lo[i];
+    total += len ? (len + O_IV_CHUNK - 1) / O_IV_CHUNK : 1;
+  }
+  first_chunk[n] = total;
+  uint32_t* owner = (uint32_t*)malloc((size_t)(total ? total : 1) * sizeof(uint32_t));
+  for (uint32_t i = 0; i < n; i++)
+    for (uint64_t c = first_chunk[i]; c < first_chunk[i + 1]; c++) owner[c] = i;
+  o_acc* acc = (o_acc*)calloc((size_t)(total ? total : 1), sizeof(o_acc));
 #ifdef _OPENMP
   if (threads > 0) omp_set_num_threads(threads);
 #pragma omp parallel for schedule(dynamic, 1)
 #endif
-  for (int64_t i = 0; i < (int64_t)n; i++) {
-    o_acc a;
-    o_acc_init(&a, 0, 0, 1);
-    o_sieve_span(&a, lo[i], hi[i], bp, nbp);
+  for (int64_t c = 0; c < (int64_t)total; c++) {
+    uint32_t i = owner[c];
+    uint64_t a = lo[i] + (uint64_t)(c - (int64_t)first_chunk[i]) * O_IV_CHUNK;
+    uint64_t b = hi[i] - a > O_IV_CHUNK ? a + O_IV_CHUNK : hi[i];
+    o_acc_init(&acc[c], 0, 0, 1);
+    o_sieve_span(&acc[c], a, b, bp, nbp);
+  }
+  for (uint32_t i = 0; i < n; i++) {
+    o_acc* A = &acc[first_chunk[i]];
+    for (uint64_t c = first_chunk[i] + 1; c < first_chunk[i + 1]; c++) o_merge(A, &acc[c]);
     voss_interval_stats* s = &out[i];
     memset(s, 0, sizeof(*s));
     s->lo = lo[i];
     s->hi = hi[i];
-    s->prime_count = a.count;
-    s->first_prime = a.first;
-    s->last_prime = a.last;
-    s->max_gap = a.max_gap;
-    s->max_gap_lo = a.max_gap_lo;
-    s->gap_overflow = a.gap_overflow;
-    memcpy(s->gap_hist, a.gap_hist, sizeof(s->gap_hist));
-    o_acc_free(&a);
+    s->prime_count = A->count;
+    s->first_prime = A->first;
+    s->last_prime = A->last;
+    s->max_gap = A->max_gap;
+    s->max_gap_lo = A->max_gap_lo;
+    s->gap_overflow = A->gap_overflow;
+    memcpy(s->gap_hist, A->gap_hist, sizeof(s->gap_hist));
   }
+  for (uint64_t c = 0; c < total; c++) o_acc_free(&acc[c]);
+  free(acc);
+  free(owner);
+  free(first_chunk);
   free(bp);
   return VOSS_OK;
 }

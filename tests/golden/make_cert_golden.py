@@ -11,7 +11,7 @@ numba) on a small large-gap list and stores what it writes:
   cert_top20_1e9.json        its top-20 text certificates, file name -> content, each without
                              its "Generated:" time-stamp line
 
-usage: python tests/golden/make_cert_golden.py [--ref /root/reference]
+usage: python tests/golden/make_cert_golden.py [--ref REFERENCE_CHECKOUT]  (default: $VOSS_REF)
 """
 import argparse
 import importlib.util
@@ -27,7 +27,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("VOSS_REF"), required=not os.environ.get("VOSS_REF"))
     a = ap.parse_args()
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     sys.path.insert(0, os.path.join(ROOT, "voss-prime-gaps_v1_b200"))

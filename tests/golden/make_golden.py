@@ -10,7 +10,7 @@ Reads (never copies wholesale) the reference's committed known answers:
   results/chebyshev.csv, hl_trend.csv   the N = 1e14 artifacts
 and writes them as compact fixtures that the tests read on machines without the reference.
 
-usage: python tests/golden/make_golden.py [--ref /root/reference]
+usage: python tests/golden/make_golden.py [--ref REFERENCE_CHECKOUT]  (default: $VOSS_REF)
 """
 import argparse
 import csv
@@ -24,7 +24,7 @@ SUP = str.maketrans("⁰¹²³⁴⁵⁶⁷⁸⁹", "0123456789")
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("VOSS_REF"), required=not os.environ.get("VOSS_REF"))
     a = ap.parse_args()
     ref = a.ref
     out = {}

@@ -91,3 +91,30 @@ def test_voss_verify_dropin_matches_reference_verifier():
             assert rr.returncode == 1
             assert open(os.path.join(res, "details_ref.csv")).read() == open(os.path.join(res, "details_ours.csv")).read()
             assert open(os.path.join(res, "cache_ref.csv")).read() == open(os.path.join(res, "cache_ours.csv")).read()
+
+
+def test_voss_master_sieves_once_whatever_the_large_gap_count(monkeypatch):
+    """The drop-in's checkpointed run returns the large-gap list up to the reference's cap in
+    one pass: no second sieve of [1, n] when the list outgrows a first guess.  With the cap
+    set below the count, the list is cut at the cap as the reference cuts it at
+    MAX_LARGE_GAPS (src/voss_v7_live.cu:292-294,809) and the count still reports all."""
+    sys.path.insert(0, os.path.join(PKG, "voss"))
+    import voss
+    import voss_master as VM
+
+    def no_second_sieve(*a, **k):
+        raise AssertionError("voss_master sieved the range a second time")
+    monkeypatch.setattr(voss.Context, "sieve_range", no_second_sieve)
+    monkeypatch.setattr(voss.Context, "sieve_range_device", no_second_sieve)
+    n = 10**9
+    with tempfile.TemporaryDirectory() as d:
+        full = VM.run(n=n, seg_num=30_000_000_000, results=d)["result"]
+        assert full.prime_count == 50847534
+        assert full.large.size == full.large_total == 296
+    with tempfile.TemporaryDirectory() as d:
+        cut = VM.run(n=n, seg_num=30_000_000_000, results=d, large_cap=100)["result"]
+        assert cut.large_total == full.large_total and cut.large.size == 100
+        rows = open(os.path.join(d, "large_gaps.csv")).read().strip().splitlines()
+        assert len(rows) == 1 + 100
+    ref = {(int(p), int(g)) for p, g in zip(full.large["position"], full.large["gap"])}
+    assert {(int(p), int(g)) for p, g in zip(cut.large["position"], cut.large["gap"])} <= ref

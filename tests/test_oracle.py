@@ -191,6 +191,26 @@ def test_oracle_intervals_and_primes():
         np.testing.assert_array_equal(O.primes_range(int(lo[i]), int(hi[i])), np.array(ps, dtype=np.uint64))
 
 
+def test_oracle_long_intervals_split_into_chunks():
+    """Intervals longer than the oracle's 2^24-integer chunk are sieved chunk by chunk in
+    parallel and merged with the gaps across the seams: the statistics equal the range
+    oracle's (one accumulator per thread span) and pi(10^9) from the reference's table."""
+    lo = np.array([0, 10**9 - 3 * 2**24 - 5, 10**12 - 5 * 10**7], dtype=np.uint64)
+    hi = np.array([10**9, 10**9 + 2**24 + 11, 10**12 + 7], dtype=np.uint64)
+    out = O.sieve_intervals(lo, hi)
+    assert out["prime_count"][0] == 50_847_534
+    for i in range(lo.size):
+        r = O.sieve_range(int(lo[i]), int(hi[i]))
+        assert out["prime_count"][i] == r.prime_count
+        assert (out["first_prime"][i], out["last_prime"][i]) == (r.first_prime, r.last_prime)
+        assert (out["max_gap"][i], out["max_gap_lo"][i]) == (r.max_gap, r.max_gap_lo)
+        want = np.zeros(1024, dtype=np.uint64)
+        for g, c in enumerate(r.gap_hist):
+            if c:
+                want[g >> 1] += c
+        np.testing.assert_array_equal(out["gap_hist"][i], want)
+
+
 needs_ref = pytest.mark.skipif(not os.path.exists(O.REF_VERIFY_SO),
                                reason="oracle/_ref/libref_verify.so not built (reference tree absent)")
 

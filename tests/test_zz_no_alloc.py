@@ -1,15 +1,20 @@
 """voss_mr_verify_noalloc: Miller-Rabin for callers that cannot allocate device memory.
 
-It must return exactly the verdicts of the allocating entry point voss_mr_verify_device.  The
+It must return exactly the verdicts of the allocating entry point voss_mr_verify_device, and a
+seeded sample of them must equal the reference verifier's is_prime_u64 (compiled unmodified;
+the oracle's restatement where that build is absent).  The
 check runs on two calls in a row because every call shares the library's fixed scratch array
 (the survivor work list and its counter): the second call must not see the first one's
 leftovers.  This file is named to be collected last, so a run that stops at the first failure
 has already run every other test; it also passes alone in a fresh process.
 """
 import ctypes
+import os
 
 import numpy as np
 import pytest
+
+import oracle_lib as O
 
 pytestmark = pytest.mark.gpu
 
@@ -52,6 +57,9 @@ def test_noalloc_matches_allocating_entry_point():
         g = got.cpu().numpy()
         assert set(np.unique(g)) <= {0, 1}
         assert int(g.sum()) >= count // 2  # the known primes are all reported prime
+        sample = rng.choice(count, 200_000, replace=False)
+        ref = O.ref_mr_batch(n[sample]) if os.path.exists(O.REF_VERIFY_SO) else O.mr_batch(n[sample])
+        np.testing.assert_array_equal(g[sample], ref)
 
 
 def test_noalloc_rejects_oversize_and_null():

@@ -72,9 +72,15 @@ def detect_gpu():
     return gpu, mem_gb, "sm_100a"
 
 
-def run(n: int = None, seg_num: int = None, results: str = None, device: int = 0) -> dict:
+def run(n: int = None, seg_num: int = None, results: str = None, device: int = 0,
+        large_cap: int = MAX_LARGE_GAPS) -> dict:
     """Sieve [1, n] in reference-compat mode, write the artifacts into `results`, print the
-    reference's report; returns {"prime_count", "total_s", "result"}."""
+    reference's report; returns {"prime_count", "total_s", "result"}.
+
+    The large-gap list keeps at most `large_cap` records, the reference's MAX_LARGE_GAPS
+    (src/voss_v7_live.cu:34,292-294,809): the checkpointed run returns the whole list up to
+    that cap in one pass (its host buffer is only touched where records are written), so
+    [1, n] is sieved once whatever the number of large gaps."""
     voss = _import_voss()
     from voss.report import WRITTEN, report_lines
     n = N_VALUE if n is None else n
@@ -86,9 +92,9 @@ def run(n: int = None, seg_num: int = None, results: str = None, device: int = 0
     with voss.Context(n + 1, device=device) as ctx:
         # segment by segment with checkpoint.bin / stop.txt in the results directory, as the
         # reference program keeps them in its working directory (src/voss_v7_live.cu:407-421,599-621)
-        cap = 1 << 22
         try:
-            res, resumed = ctx.run_checkpointed(n, seg_num, compat=True, ckpt_every=5, directory=results, large_cap=cap)
+            res, resumed = ctx.run_checkpointed(n, seg_num, compat=True, ckpt_every=5, directory=results,
+                                                large_cap=large_cap)
         except voss.VossError as e:
             if e.code == -7:  # stop file: checkpoint saved, clean exit (:603-620)
                 print(f"\n>>> STOP-FILE detected — exiting cleanly <<<")
@@ -98,9 +104,6 @@ def run(n: int = None, seg_num: int = None, results: str = None, device: int = 0
             print(f">>> RESUMING FROM SEGMENT {resumed} / {num_seg} <<<")
         else:
             print(">>> STARTING FRESH <<<")
-        if res.large_total > cap:
-            cap = min(int(res.large_total), MAX_LARGE_GAPS)
-            res = ctx.sieve_range(1, n + 1, compat=True, seg_num=seg_num, large_cap=cap)
         t_sieve = time.perf_counter() - t0
         gap, p = ctx.gap_sequence(n, seg_num, GAP_SEQ_SIZE)
     total_s = time.perf_counter() - t0

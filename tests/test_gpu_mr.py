@@ -134,3 +134,38 @@ def test_prove_gaps_large_batches_through_staging(gpu_ctx):
     sel = np.arange(0, p.size, 997)
     ref = O.ref_prove_gaps(p[sel], g[sel]) if os.path.exists(O.REF_VERIFY_SO) else O.prove_gaps(p[sel], g[sel])
     np.testing.assert_array_equal(got[sel], ref)
+
+
+def test_staging_in_many_chunks_equals_direct_copies(monkeypatch):
+    """With the staging buffers limited to 2^17 entries (VOSS_STAGE_LIMIT, read when a context is
+    created) every staged transfer crosses in many chunks that alternate between the two
+    buffers: Miller-Rabin candidates in and verdicts out, gap proofs in and out, and interval
+    results out.  Each result equals the same work in batches small enough to be copied
+    directly."""
+    import voss
+    monkeypatch.setenv("VOSS_STAGE_LIMIT", str(1 << 17))
+    rng = np.random.default_rng(31)
+    with voss.Context(10**12) as ctx:
+        n = rng.integers(0, 2**63, size=3 * 2**20 + 5, dtype=np.uint64) * 2 + 1
+        n[::89] = rng.integers(0, 10**9, size=n[::89].size, dtype=np.uint64)
+        got = ctx.mr_verify(n)
+        step = (1 << 20) - 1
+        np.testing.assert_array_equal(got, np.concatenate([ctx.mr_verify(n[i:i + step])
+                                                           for i in range(0, n.size, step)]))
+        sel = np.arange(0, n.size, 101)
+        np.testing.assert_array_equal(got[sel], checker(n[sel]))
+        gaps = ctx.gaps_at_least(1, 3 * 10**9, 90)
+        assert gaps.size > (1 << 20)
+        p = gaps["position"].astype(np.uint64)
+        g = gaps["gap"].astype(np.int32)
+        g[::7] += 2
+        ok = ctx.prove_gaps(p, g)
+        np.testing.assert_array_equal(ok, np.concatenate([ctx.prove_gaps(p[i:i + step], g[i:i + step])
+                                                          for i in range(0, p.size, step)]))
+        assert not ok[::7].any() and ok[1::7].all()
+        lo = (10 ** rng.uniform(3, 11, 1500)).astype(np.uint64)
+        hi = lo + (10 ** rng.uniform(0, 4, lo.size)).astype(np.uint64)
+        big = ctx.sieve_intervals(lo, hi)                 # 12 MB of results: staged, 12 chunks
+        small = np.concatenate([ctx.sieve_intervals(lo[i:i + 500], hi[i:i + 500]) for i in range(0, lo.size, 500)])
+        for f in voss.INTERVAL_DTYPE.names:
+            np.testing.assert_array_equal(big[f], small[f], err_msg=f)

@@ -236,3 +236,21 @@ def test_large_interval_batches_through_staging(gpu_ctx):
     _same_intervals(big, small)
     sel = np.arange(0, k, 37)
     _same_intervals(big[sel], O.sieve_intervals(lo[sel], hi[sel]))
+
+
+def test_intervals_at_the_top_of_the_supported_range():
+    """Intervals just below 2^62 (the largest max_hi a context takes): base primes up to 2^31,
+    so the large-prime pre-pass meets primes of 2^30 and more, whose remainders take its 64-bit
+    form.  Sieved (Miller-Rabin route off) and routed, both equal to the oracle."""
+    import voss
+    top = 1 << 62
+    lo = np.array([top - 10**6, top - 3 * 10**5 - 17, top - 2 * 10**7], dtype=np.uint64)
+    hi = np.array([top, top - 10**5, top - 2 * 10**7 + 4 * 10**5], dtype=np.uint64)
+    want = O.sieve_intervals(lo, hi)
+    with voss.Context(top) as ctx:
+        t0 = ctx.tuning()
+        routed = ctx.sieve_intervals(lo, hi)
+        ctx.set_tuning(**{**t0, "mr_route": 0xFFFFFFFF})
+        sieved = ctx.sieve_intervals(lo, hi)
+    _same_intervals(sieved, want)
+    _same_intervals(routed, want)

@@ -8,7 +8,9 @@
 //                masks the interval's ends (the reference's cudaMemset + first-word patch, :496-500);
 //   2. sieve:    clears the odd multiples of the base primes 37 <= p <= isqrt(hi-1)
 //                (the reference's sieve_w30_seg_kernel, :120-143, one launch per prime):
-//                  small primes  p <  tile_bytes/coop_div : one warp per prime, lanes stride 32p,
+//                  small primes  p <  tile_bytes/coop_div : one warp per prime, each residue
+//                                                            progression split over the lanes in
+//                                                            blocks of 4 hits (no bank conflicts),
 //                  medium primes p <  mult_factor*tile_bytes: one thread per prime, 8 residues,
 //                  large primes  otherwise                 : one thread per prime, walking its
 //                                                            multiples across the tile's span;
@@ -125,26 +127,35 @@ __device__ __forceinline__ void clear_bit_word(uint32_t* bm, uint32_t word, uint
   atomicAnd(bm + word, mask);
 }
 
-// Clears bit `bit` of every byte start, start + 4 ws, start + 8 ws, ... below Lt (one lane of a
-// warp-cooperative small prime; the stride is 4 ws bytes = ws words).  The stride is a multiple of
-// 4 bytes, so the byte lane inside the word, and with it the mask, never changes; four clears per
-// loop trip.
-__device__ __forceinline__ void clear_lane_progression(uint32_t* bm, uint32_t start, uint32_t ws,
-                                                       uint32_t bit, uint32_t Lt, uint32_t nw,
-                                                       uint32_t* err) {
-  const uint32_t mask = ~(1u << (((start & 3u) << 3) | bit));
-  const uint32_t wlim = (Lt + 3u - (start & 3u)) >> 2;  // start + 4k < Lt  <=>  (start >> 2) + k < wlim
-  uint32_t w = start >> 2;
-  if (wlim > 3u * ws) {
-    const uint32_t wlim4 = wlim - 3u * ws;
-    for (; w < wlim4; w += 4u * ws) {
-      clear_bit_word(bm, w, mask, nw, err);
-      clear_bit_word(bm, w + ws, mask, nw, err);
-      clear_bit_word(bm, w + 2u * ws, mask, nw, err);
-      clear_bit_word(bm, w + 3u * ws, mask, nw, err);
+// One lane's share of a warp-cooperative residue progression bytes s, s + p, s + 2p, ... (p odd):
+// lane m clears the hits 4m + 128t + u (u = 0..3, t >= 0), i.e. bytes
+// byte + u p + 128 p t with byte = s + 4 p m, all below Lt.  For a fixed (t, u) the 32 lanes'
+// words are c + p m + 32 p t with c = (s + u p) >> 2 common to the warp: as p is odd they fall
+// in 32 distinct banks, so every shared-memory atomic of the warp is a single wavefront.  The
+// lane's four bytes of a block lie in four distinct byte lanes of their words and a block
+// advances by 128 p bytes = 32 p words, so the four masks and word offsets stay fixed.
+__device__ __forceinline__ void clear_block_progression(uint32_t* bm, uint32_t byte, uint32_t p, uint32_t bit,
+                                                        uint32_t Lt, uint32_t nw, uint32_t* err) {
+  if (byte + 3u * p < Lt) {
+    const uint32_t b1 = byte + p, b2 = b1 + p, b3 = b2 + p;
+    const uint32_t m0 = ~(1u << (((byte & 3u) << 3) | bit)), m1 = ~(1u << (((b1 & 3u) << 3) | bit));
+    const uint32_t m2 = ~(1u << (((b2 & 3u) << 3) | bit)), m3 = ~(1u << (((b3 & 3u) << 3) | bit));
+    uint32_t w0 = byte >> 2;
+    const uint32_t d1 = (b1 >> 2) - w0, d2 = (b2 >> 2) - w0, d3 = (b3 >> 2) - w0;
+    const uint32_t ws = 32u * p;
+    // b3 + 128 p k < Lt  <=>  (b3 >> 2) + 32 p k < lim
+    const uint32_t lim = ((Lt + 3u - (b3 & 3u)) >> 2) - d3;
+    uint32_t k = 0;
+    for (; w0 < lim; w0 += ws, ++k) {
+      clear_bit_word(bm, w0, m0, nw, err);
+      clear_bit_word(bm, w0 + d1, m1, nw, err);
+      clear_bit_word(bm, w0 + d2, m2, nw, err);
+      clear_bit_word(bm, w0 + d3, m3, nw, err);
     }
+    byte += 128u * p * k;
   }
-  for (; w < wlim; w += ws) clear_bit_word(bm, w, mask, nw, err);
+  // at most three hits remain (byte + 3p >= Lt); the next block belongs to the next lane
+  for (; byte < Lt; byte += p) clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
 }
 
 // Clears bit `bit` of bytes byte, byte + p, byte + 2p, ... below Lt (p odd).  Four consecutive
@@ -362,10 +373,6 @@ __device__ __forceinline__ uint32_t acc_index(uint32_t i) {
   return (uint32_t)kAccCls143 + 8u * (c >= 143u ? c - 143u : c) + (i & 7u);
 }
 
-// Warp-cooperative primes p >= tile bytes / kSmallSplitDiv give each residue 4 lanes; smaller
-// ones give each residue all 32 lanes in turn.
-constexpr uint32_t kSmallSplitDiv = 512;
-
 constexpr uint32_t kFlushEvery = 2048;  // tiles between counter flushes (u32 headroom)
 
 template <int BLOCK, bool EMIT>
@@ -531,8 +538,9 @@ sieve_tiles_kernel(SieveArgs a) {
     {
       const uint64_t ktile = H.ktile;
       const uint32_t ia = H.ia, ib = H.ib, iw = H.iw, np = H.np;
-      // small primes: a warp per prime
-      const uint32_t split = Lt / kSmallSplitDiv;
+      // small primes: a warp per prime, its eight residue progressions in turn, each split over
+      // the lanes in blocks of four consecutive hits (bank-conflict-free, clear_block_progression)
+      const uint32_t lane_ofs = 4u * (uint32_t)lane;
       for (;;) {
         uint32_t i = 0;
         if (lane == 0) i = atomicAdd(&H.coop_ctr, 1u);
@@ -541,22 +549,13 @@ sieve_tiles_kernel(SieveArgs a) {
         const uint32_t p = a.primes[i];
         const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
         const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
-        if (p >= split) {
-          // 4 lanes per residue progression (lane = 4 o + q: bytes s_o + q p + 4p k)
-          const uint32_t o = (uint32_t)lane >> 2;
+        const uint32_t lp = lane_ofs * p;
+#pragma unroll 1
+        for (uint32_t o = 0; o < 8; ++o) {
           const uint32_t e = s_step[bi * 8u + o];
           const uint32_t delta = pa * w30(o) + (e & 31u);
           const uint32_t s = delta >= r ? delta - r : delta + p - r;
-          clear_lane_progression(bm, s + ((uint32_t)lane & 3u) * p, p, e >> 5, Lt, nw, err);
-        } else {
-          // all 32 lanes on one residue progression, residues in turn (lane q: bytes s_o + q p + 32p k)
-#pragma unroll 1
-          for (uint32_t o = 0; o < 8; ++o) {
-            const uint32_t e = s_step[bi * 8u + o];
-            const uint32_t delta = pa * w30(o) + (e & 31u);
-            const uint32_t s = delta >= r ? delta - r : delta + p - r;
-            clear_lane_progression(bm, s + (uint32_t)lane * p, 8u * p, e >> 5, Lt, nw, err);
-          }
+          clear_block_progression(bm, s + lp, p, e >> 5, Lt, nw, err);
         }
       }
       VOSS_PHASE(3)
@@ -935,7 +934,7 @@ int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_int
 // them in the launch's large-prime bitmap with global atomics.  The prime table is read once
 // per launch instead of once per tile, which is what bounds high intervals (at 1e18 the table
 // is 610 MB).  The tile kernel ANDs this bitmap into its fill and skips these primes.
-constexpr int kScatterChunk = 1024;  // 40 KB of interval descriptors per block
+constexpr int kScatterChunk = 960;  // 45 KB of interval descriptors per block
 
 __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __restrict__ primes,
                                                             const uint64_t* __restrict__ magic, uint32_t j0,
@@ -956,22 +955,34 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
     const double inv = 1.0 / (double)p;
     const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
     const uint8_t* row = s_wstep + bi * 8u;
+    const bool narrow = p < (1u << 30);
     for (uint32_t s = 0; s < n_iv; ++s) {
-      const IntervalScatter I = s_iv[s];
-      if (p > I.sqrt_hi) break;
-      const uint32_t r = mod_by_estimate(I.vbase, I.vbase_d, p, inv);
-      const uint64_t d = r ? (uint64_t)(p - r) : 0ull;  // first multiple of p, offset from vbase
-      if (d >= I.span) continue;                         // none in the interval
-      const uint64_t lt = I.span / 30ull;                // bytes of the interval's bitmap
-      if (lt < (1ull << 31)) {
+      // vbase mod p from the truncated quotient estimate q (within one of floor(vbase / p), as in
+      // mod_by_estimate): vbase - q p lies in (-p, 2p), inside the int32 range for p < 2^30, so
+      // only the low 32 bits of vbase and of q p are needed (p >= 2^30, for hi above 2^60, takes
+      // the 64-bit form)
+      const double vd = s_iv[s].vbase_d;
+      const uint2 lo_sq = *reinterpret_cast<const uint2*>(&s_iv[s].vbase_lo);  // (vbase_lo, sqrt_hi)
+      if (p > lo_sq.y) break;
+      const unsigned long long q = __double2ull_rz(vd * inv);
+      int64_t rr;
+      if (narrow) rr = (int32_t)(lo_sq.x - (uint32_t)q * p);
+      else rr = (int64_t)(s_iv[s].vbase - q * (uint64_t)p);
+      rr += rr < 0 ? (int64_t)p : 0;
+      rr -= rr >= (int64_t)p ? (int64_t)p : 0;
+      const uint32_t d = rr ? p - (uint32_t)rr : 0u;  // first multiple of p, offset from vbase
+      const uint2 sp_lt = *reinterpret_cast<const uint2*>(&s_iv[s].span32);  // (span32, lt32)
+      if (d >= sp_lt.x) continue;                      // none in the interval
+      const IntervalScatter& I = s_iv[s];
+      if (sp_lt.y) {
         // wheel walk over the multiples p*m with gcd(m, 30) = 1 (vbase is a multiple of 30)
-        const uint32_t d32 = (uint32_t)d;
-        const uint32_t st = s_wstart[bi * 30u + (d32 - 30u * (d32 / 30u))];
-        const uint64_t off = d + (uint64_t)(st & 7u) * p;
+        const uint32_t st = s_wstart[bi * 30u + (d - 30u * (d / 30u))];
+        const uint64_t off = (uint64_t)d + (uint64_t)(st & 7u) * p;
         if (off >= I.span) continue;
         uint32_t byte = (uint32_t)(off / 30ull), w = st >> 3;
+        const uint32_t lt = sp_lt.y;
         uint32_t* g = gbm + I.gword;
-        while (byte < (uint32_t)lt) {
+        while (byte < lt) {
           const uint32_t e = row[w];
           atomicAnd(g + (byte >> 2), ~(1u << (((byte & 3u) << 3) | (e & 7u))));
           byte += pa * ((e >> 5) & 6u) + ((e >> 3) & 7u);
@@ -979,9 +990,9 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
         }
       } else {
         for (uint64_t dd = d; dd < I.span; dd += p) {
-          const uint64_t q = dd / 30ull;
-          const int b = s_rb[(uint32_t)(dd - 30ull * q)];
-          if (b >= 0) atomicAnd(gbm + I.gword + (q >> 2), ~(1u << ((((uint32_t)q & 3u) << 3) | (uint32_t)b)));
+          const uint64_t q64 = dd / 30ull;
+          const int b = s_rb[(uint32_t)(dd - 30ull * q64)];
+          if (b >= 0) atomicAnd(gbm + I.gword + (q64 >> 2), ~(1u << ((((uint32_t)q64 & 3u) << 3) | (uint32_t)b)));
         }
       }
     }

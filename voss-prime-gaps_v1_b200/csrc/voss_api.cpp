@@ -12,7 +12,9 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <string>
 #include <thread>
 #include <vector>
@@ -267,8 +269,10 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
       I.span = 120ull * d.n_words;
       I.gword = d.gword;
       I.sqrt_hi = (uint32_t)std::min<uint64_t>(sq, 0xFFFFFFFFull);
-      I.pad = 0;
       I.vbase_d = (double)I.vbase;
+      I.vbase_lo = (uint32_t)I.vbase;
+      I.span32 = (uint32_t)std::min<uint64_t>(I.span, 0xFFFFFFFFull);
+      I.lt32 = I.span / 30 < (1ull << 31) ? (uint32_t)(I.span / 30) : 0u;
       sc.push_back(I);
       wbytes += 4ull * d.n_words;
       wins.back().n++;
@@ -325,7 +329,7 @@ int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_c
 }
 
 // memcpy split over host threads: one thread copies from pageable memory at a fraction of the
-// host's memory bandwidth.
+// host's memory bandwidth.  A part whose thread cannot be started is copied by the caller.
 void parallel_copy(void* dst, const void* src, size_t bytes) {
   const size_t kMinPart = 8u << 20;
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
@@ -336,20 +340,31 @@ void parallel_copy(void* dst, const void* src, size_t bytes) {
   }
   const size_t step = (bytes / parts + 63) & ~(size_t)63;
   std::vector<std::thread> th;
+  th.reserve(parts);
   for (size_t i = 1; i < parts; ++i) {
     const size_t a = std::min(bytes, i * step), b = std::min(bytes, (i + 1) * step);
-    if (a < b)
+    if (a >= b) continue;
+    try {
       th.emplace_back([=] { std::memcpy((char*)dst + a, (const char*)src + a, b - a); });
+    } catch (const std::exception&) {
+      std::memcpy((char*)dst + a, (const char*)src + a, b - a);
+    }
   }
   std::memcpy(dst, src, std::min(bytes, step));
   for (auto& t : th) t.join();
 }
 
-// The context's two pinned staging buffers, at least `entries` 64-bit words each (grow-only).
+// The context's two pinned staging buffers, ready for host writes: every transfer that may
+// still use them (left queued by an earlier call that returned early) has finished.  They hold
+// min(entries, stage_limit) 64-bit words each (grow-only); callers move data in chunks of
+// h_stage_cap words.
 int ensure_stage(voss_ctx* c, size_t entries) {
+  entries = std::max<size_t>(1, std::min(entries, c->stage_limit));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
+  for (int b = 0; b < 2; ++b) CUDA_TRY(cudaEventSynchronize(c->ev_stage[b]));
   if (entries <= c->h_stage_cap) return VOSS_OK;
   for (int b = 0; b < 2; ++b) {
-    CUDA_TRY(cudaEventSynchronize(c->ev_stage[b]));
     if (c->h_stage[b]) cudaFreeHost(c->h_stage[b]);
     c->h_stage[b] = nullptr;
   }
@@ -360,6 +375,48 @@ int ensure_stage(voss_ctx* c, size_t entries) {
       return fail(VOSS_ERR_NOMEM, "cudaMallocHost of the staging buffers failed");
     }
   c->h_stage_cap = entries;
+  return VOSS_OK;
+}
+
+// Host -> device through the staging buffers on stream s: chunk i is filled by host threads
+// into buffer i & 1 once that buffer's previous transfer is done, then crosses while chunk
+// i + 1 is filled.  Returns once the last chunk is queued.
+int stage_in(voss_ctx* c, void* d_dst, const void* src, size_t bytes, cudaStream_t s) {
+  const size_t chunk = c->h_stage_cap * sizeof(uint64_t);
+  size_t i = 0;
+  for (size_t off = 0; off < bytes; off += chunk, ++i) {
+    const size_t k = std::min(chunk, bytes - off);
+    const int b = (int)(i & 1);
+    CUDA_TRY(cudaEventSynchronize(c->ev_stage[b]));
+    parallel_copy(c->h_stage[b], (const char*)src + off, k);
+    CUDA_TRY(cudaMemcpyAsync((char*)d_dst + off, c->h_stage[b], k, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaEventRecord(c->ev_stage[b], s));
+  }
+  return VOSS_OK;
+}
+
+// Device -> host through the staging buffers, after the work queued on s: chunk j crosses into
+// buffer j & 1 while host threads copy chunk j - 1 out.  Returns with every byte in dst.
+int stage_out(voss_ctx* c, void* dst, const void* d_src, size_t bytes, cudaStream_t s) {
+  const size_t chunk = c->h_stage_cap * sizeof(uint64_t);
+  size_t prev_off = 0, prev_k = 0, j = 0;
+  for (size_t off = 0; off < bytes; off += chunk, ++j) {
+    const size_t k = std::min(chunk, bytes - off);
+    const int b = (int)(j & 1);
+    CUDA_TRY(cudaEventSynchronize(c->ev_stage[b]));  // nothing of this buffer is still crossing in
+    CUDA_TRY(cudaMemcpyAsync(c->h_stage[b], (const char*)d_src + off, k, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaEventRecord(c->ev_stage[b], s));
+    if (j > 0) {
+      CUDA_TRY(cudaEventSynchronize(c->ev_stage[b ^ 1]));
+      parallel_copy((char*)dst + prev_off, c->h_stage[b ^ 1], prev_k);
+    }
+    prev_off = off;
+    prev_k = k;
+  }
+  if (j > 0) {
+    CUDA_TRY(cudaEventSynchronize(c->ev_stage[(j - 1) & 1]));
+    parallel_copy((char*)dst + prev_off, c->h_stage[(j - 1) & 1], prev_k);
+  }
   return VOSS_OK;
 }
 
@@ -772,6 +829,10 @@ VOSS_API int voss_ctx_create(int device, uint64_t max_hi, voss_ctx** out) {
     return bail(fail(VOSS_ERR_CUDA, "presieve table upload failed"));
   voss_tuning t{};
   if ((rc = apply_tuning(c, t))) return bail(rc);
+  if (const char* lim = std::getenv("VOSS_STAGE_LIMIT")) {
+    const unsigned long long v = std::strtoull(lim, nullptr, 10);
+    if (v) c->stage_limit = std::max<size_t>(1024, (size_t)v);
+  }
   *out = c;
   return VOSS_OK;
 }
@@ -914,16 +975,16 @@ VOSS_API int voss_sieve_intervals(voss_ctx* c, const uint64_t* lo, const uint64_
   uint32_t ctr[kCtrWords];
   CUDA_TRY(cudaMemcpyAsync(ctr, W.counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, s));
   // large results (8 KB per interval) come back through pinned staging, copied out by host threads
+  // (two halves over the two buffers: the second crosses while the first is copied out)
   const size_t res_bytes = sizeof(voss_interval_stats) * n;
   const bool staged = res_bytes >= (8u << 20);
   if (staged) {
-    if ((rc = ensure_stage(c, res_bytes / sizeof(uint64_t) + 1))) return rc;
-    CUDA_TRY(cudaMemcpyAsync(c->h_stage[0], W.istats.p, res_bytes, cudaMemcpyDeviceToHost, s));
+    if ((rc = ensure_stage(c, (res_bytes + 15) / 16))) return rc;
+    if ((rc = stage_out(c, out, W.istats.p, res_bytes, s))) return rc;
   } else {
     CUDA_TRY(cudaMemcpyAsync(out, W.istats.p, res_bytes, cudaMemcpyDeviceToHost, s));
   }
   CUDA_TRY(cudaStreamSynchronize(s));
-  if (staged) parallel_copy(out, c->h_stage[0], res_bytes);
   if ((rc = check_device_error(ctr))) return rc;
   cudaEventElapsedTime(&c->sieve_ms, c->ev0, c->ev1);
   cudaEventElapsedTime(&c->total_ms, c->ev0, c->ev2);
@@ -1039,13 +1100,13 @@ VOSS_API int voss_mr_verify(voss_ctx* c, const uint64_t* n, uint64_t count, uint
   // through two pinned staging buffers that host threads fill (chunk i + 1 is copied in while
   // chunk i crosses and chunk i - 1 is tested), and the verdicts come back the same way; small
   // ones are copied straight from the caller's memory.
-  constexpr uint64_t kChunk = 1ull << 24;
-  const uint64_t per = std::min(count, kChunk);
   const bool staged = count >= (1ull << 20);
+  if (staged && (rc = ensure_stage(c, std::min<uint64_t>(count, 1ull << 24)))) return rc;
+  const uint64_t kChunk = staged ? c->h_stage_cap : (1ull << 24);  // candidates per launch
+  const uint64_t per = std::min(count, kChunk);
   if ((rc = W.mr_in.ensure(count * 8)) || (rc = W.mr_out.ensure(count)) ||
       (rc = W.mr_work.ensure(sizeof(uint32_t) * (per + 8))))
     return rc;
-  if (staged && (rc = ensure_stage(c, per))) return rc;
   uint64_t* d_in = W.mr_in.as<uint64_t>();
   uint8_t* d_out = W.mr_out.as<uint8_t>();
   uint32_t* work = W.mr_work.as<uint32_t>();
@@ -1073,23 +1134,7 @@ VOSS_API int voss_mr_verify(voss_ctx* c, const uint64_t* n, uint64_t count, uint
   }
   // verdicts: chunk j crosses into buffer j & 1 while chunk j - 1 is copied out by host threads
   // (the input transfers are complete: every launch on `stream` waited for them)
-  const uint64_t ob = c->h_stage_cap * sizeof(uint64_t);
-  uint64_t prev_off = 0, prev_k = 0;
-  uint64_t j = 0;
-  for (uint64_t off = 0; off < count; off += ob, ++j) {
-    const uint64_t k = std::min(ob, count - off);
-    const int b = (int)(j & 1);
-    CUDA_TRY(cudaMemcpyAsync(c->h_stage[b], d_out + off, k, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaEventRecord(c->ev_stage[b], s));
-    if (j > 0) {
-      CUDA_TRY(cudaEventSynchronize(c->ev_stage[b ^ 1]));
-      parallel_copy(is_prime + prev_off, c->h_stage[b ^ 1], prev_k);
-    }
-    prev_off = off;
-    prev_k = k;
-  }
-  CUDA_TRY(cudaEventSynchronize(c->ev_stage[(j - 1) & 1]));
-  parallel_copy(is_prime + prev_off, c->h_stage[(j - 1) & 1], prev_k);
+  if ((rc = stage_out(c, is_prime, d_out, count, s))) return rc;
   CUDA_TRY(cudaStreamSynchronize(s));
   return VOSS_OK;
 }
@@ -1112,19 +1157,23 @@ VOSS_API int voss_prove_gaps(voss_ctx* c, const uint64_t* p_after, const int32_t
   // large batches cross through the pinned staging buffers (filled and emptied by host threads)
   const bool staged = count >= (1ull << 20);
   if (staged) {
-    if ((rc = ensure_stage(c, count))) return rc;
-    parallel_copy(c->h_stage[0], p_after, count * 8);
-    parallel_copy(c->h_stage[1], gap, count * 4);
+    if ((rc = ensure_stage(c, (count + 1) / 2)) || (rc = stage_in(c, W.pg_pa.p, p_after, count * 8, s)) ||
+        (rc = stage_in(c, W.pg_gap.p, gap, count * 4, s)))
+      return rc;
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(W.pg_pa.p, p_after, count * 8, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(W.pg_gap.p, gap, count * 4, cudaMemcpyHostToDevice, s));
   }
-  CUDA_TRY(cudaMemcpyAsync(W.pg_pa.p, staged ? (const void*)c->h_stage[0] : p_after, count * 8, cudaMemcpyHostToDevice, s));
-  CUDA_TRY(cudaMemcpyAsync(W.pg_gap.p, staged ? (const void*)c->h_stage[1] : gap, count * 4, cudaMemcpyHostToDevice, s));
   uint32_t* work = W.mr_work.as<uint32_t>();
   if (launch_prove_gaps(W.pg_pa.as<uint64_t>(), W.pg_gap.as<int32_t>(), count, W.pg_ok.as<uint8_t>(),
                         W.mr_in.as<uint64_t>(), W.mr_out.as<uint8_t>(), work + 8, work, s, c->sm_count))
     return fail(VOSS_ERR_CUDA, "gap proof launch failed");
-  CUDA_TRY(cudaMemcpyAsync(staged ? (void*)c->h_stage[0] : ok, W.pg_ok.p, count, cudaMemcpyDeviceToHost, s));
+  if (staged) {
+    if ((rc = stage_out(c, ok, W.pg_ok.p, count, s))) return rc;
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(ok, W.pg_ok.p, count, cudaMemcpyDeviceToHost, s));
+  }
   CUDA_TRY(cudaStreamSynchronize(s));
-  if (staged) parallel_copy(ok, c->h_stage[0], count);
   return VOSS_OK;
 }
 

@@ -131,6 +131,10 @@ struct voss_ctx {
   uint64_t* h_stage[2] = {nullptr, nullptr};
   size_t h_stage_cap = 0;  // 64-bit entries per buffer
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
+  // most 64-bit entries a staging buffer may hold (larger transfers cross in chunks); the
+  // environment variable VOSS_STAGE_LIMIT lowers it when the context is created, so tests can
+  // drive the chunked paths with small batches
+  size_t stage_limit = ~(size_t)0;
 };
 
 namespace voss_host {

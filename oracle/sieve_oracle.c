@@ -94,23 +94,61 @@ static uint64_t o_isqrt(uint64_t x) {
   return s;
 }
 
+/* All primes <= limit, ascending (the list build_base_sieve makes, verify_cpp.cpp:95-103).
+ * Small limits use the plain sieve of a byte per integer; above 2^24 the odd integers are
+ * sieved in segments of 2^21 by the primes up to sqrt(limit), so that limits near 2^31
+ * (intervals just below 2^62) take seconds rather than a minute of cache misses. */
 uint32_t* oracle_base_primes(uint64_t limit, uint64_t* count) {
-  uint8_t* s = (uint8_t*)malloc(limit + 1);
-  if (!s) { *count = 0; return NULL; }
-  memset(s, 1, limit + 1);
-  s[0] = 0;
-  if (limit >= 1) s[1] = 0;
-  for (uint64_t i = 2; i * i <= limit; i++)
-    if (s[i])
-      for (uint64_t j = i * i; j <= limit; j += i) s[j] = 0;
-  uint64_t c = 0;
-  for (uint64_t i = 2; i <= limit; i++) c += s[i];
-  uint32_t* p = (uint32_t*)malloc((c ? c : 1) * sizeof(uint32_t));
+  if (limit <= (1u << 24)) {
+    uint8_t* s = (uint8_t*)malloc(limit + 1);
+    if (!s) { *count = 0; return NULL; }
+    memset(s, 1, limit + 1);
+    s[0] = 0;
+    if (limit >= 1) s[1] = 0;
+    for (uint64_t i = 2; i * i <= limit; i++)
+      if (s[i])
+        for (uint64_t j = i * i; j <= limit; j += i) s[j] = 0;
+    uint64_t c = 0;
+    for (uint64_t i = 2; i <= limit; i++) c += s[i];
+    uint32_t* p = (uint32_t*)malloc((c ? c : 1) * sizeof(uint32_t));
+    uint64_t k = 0;
+    for (uint64_t i = 2; i <= limit; i++)
+      if (s[i]) p[k++] = (uint32_t)i;
+    free(s);
+    *count = c;
+    return p;
+  }
+  uint64_t nsm = 0;
+  uint32_t* sm = oracle_base_primes(o_isqrt(limit), &nsm);
+  /* pi(x) < 1.26 x / ln x for x > 1 (Rosser-Schoenfeld): capacity for the whole list */
+  uint64_t cap = (uint64_t)(1.26 * (double)limit / log((double)limit)) + 64;
+  uint32_t* p = (uint32_t*)malloc(cap * sizeof(uint32_t));
+  const uint64_t SEG = 1u << 21; /* odd integers per segment */
+  uint8_t* seg = (uint8_t*)malloc(SEG);
+  if (!p || !seg || !sm) { free(p); free(seg); free(sm); *count = 0; return NULL; }
   uint64_t k = 0;
-  for (uint64_t i = 2; i <= limit; i++)
-    if (s[i]) p[k++] = (uint32_t)i;
-  free(s);
-  *count = c;
+  p[k++] = 2;
+  for (uint64_t base = 1; base <= limit; base += 2 * SEG) { /* slot i <-> base + 2i */
+    uint64_t n = SEG;
+    if (base + 2 * (n - 1) > limit) n = (limit - base) / 2 + 1;
+    memset(seg, 1, n);
+    const uint64_t vmax = base + 2 * (n - 1);
+    for (uint64_t t = 1; t < nsm; t++) { /* odd primes */
+      const uint64_t q = sm[t];
+      if (q * q > vmax) break;
+      uint64_t m = q * q;
+      if (m < base) {
+        m = (base + q - 1) / q * q;
+        if ((m & 1) == 0) m += q;
+      }
+      for (uint64_t i = (m - base) / 2; i < n; i += q) seg[i] = 0;
+    }
+    for (uint64_t i = 0; i < n; i++)
+      if (seg[i] && base + 2 * i > 1) p[k++] = (uint32_t)(base + 2 * i);
+  }
+  free(seg);
+  free(sm);
+  *count = k;
   return p;
 }
 

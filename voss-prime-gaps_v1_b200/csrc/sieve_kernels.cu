@@ -8,9 +8,11 @@
 //                masks the interval's ends (the reference's cudaMemset + first-word patch, :496-500);
 //   2. sieve:    clears the odd multiples of the base primes 37 <= p <= isqrt(hi-1)
 //                (the reference's sieve_w30_seg_kernel, :120-143, one launch per prime):
-//                  small primes  p <  tile_bytes/coop_div : one warp per prime, each residue
-//                                                            progression split over the lanes in
-//                                                            blocks of 4 hits (no bank conflicts),
+//                  small primes  p <  tile_bytes/coop_div : one warp per prime: below
+//                                                            tile_bytes/512 each residue progression
+//                                                            split over all lanes in blocks of 4
+//                                                            hits (no bank conflicts), above it 4
+//                                                            lanes per residue,
 //                  medium primes p <  mult_factor*tile_bytes: one thread per prime, 8 residues,
 //                  large primes  otherwise                 : one thread per prime, walking its
 //                                                            multiples across the tile's span;
@@ -125,6 +127,28 @@ __device__ __forceinline__ void clear_bit_word(uint32_t* bm, uint32_t word, uint
                                                uint32_t limit, uint32_t* err) {
   VOSS_SM_GUARD(word, limit)
   atomicAnd(bm + word, mask);
+}
+
+// Clears bit `bit` of every byte start, start + 4 ws, start + 8 ws, ... below Lt (one lane of a
+// warp-cooperative small prime; the stride is 4 ws bytes = ws words).  The stride is a multiple of
+// 4 bytes, so the byte lane inside the word, and with it the mask, never changes; four clears per
+// loop trip.
+__device__ __forceinline__ void clear_lane_progression(uint32_t* bm, uint32_t start, uint32_t ws,
+                                                       uint32_t bit, uint32_t Lt, uint32_t nw,
+                                                       uint32_t* err) {
+  const uint32_t mask = ~(1u << (((start & 3u) << 3) | bit));
+  const uint32_t wlim = (Lt + 3u - (start & 3u)) >> 2;  // start + 4k < Lt  <=>  (start >> 2) + k < wlim
+  uint32_t w = start >> 2;
+  if (wlim > 3u * ws) {
+    const uint32_t wlim4 = wlim - 3u * ws;
+    for (; w < wlim4; w += 4u * ws) {
+      clear_bit_word(bm, w, mask, nw, err);
+      clear_bit_word(bm, w + ws, mask, nw, err);
+      clear_bit_word(bm, w + 2u * ws, mask, nw, err);
+      clear_bit_word(bm, w + 3u * ws, mask, nw, err);
+    }
+  }
+  for (; w < wlim; w += ws) clear_bit_word(bm, w, mask, nw, err);
 }
 
 // One lane's share of a warp-cooperative residue progression bytes s, s + p, s + 2p, ... (p odd):
@@ -373,6 +397,13 @@ __device__ __forceinline__ uint32_t acc_index(uint32_t i) {
   return (uint32_t)kAccCls143 + 8u * (c >= 143u ? c - 143u : c) + (i & 7u);
 }
 
+// Warp-cooperative primes p >= tile bytes / kSmallSplitDiv give each residue 4 lanes (their few
+// hits per residue keep a lane's loop long); smaller ones give each residue all 32 lanes in turn.
+#ifndef VOSS_SMALL_SPLIT_DIV
+#define VOSS_SMALL_SPLIT_DIV 512
+#endif
+constexpr uint32_t kSmallSplitDiv = VOSS_SMALL_SPLIT_DIV;
+
 constexpr uint32_t kFlushEvery = 2048;  // tiles between counter flushes (u32 headroom)
 
 template <int BLOCK, bool EMIT>
@@ -538,8 +569,8 @@ sieve_tiles_kernel(SieveArgs a) {
     {
       const uint64_t ktile = H.ktile;
       const uint32_t ia = H.ia, ib = H.ib, iw = H.iw, np = H.np;
-      // small primes: a warp per prime, its eight residue progressions in turn, each split over
-      // the lanes in blocks of four consecutive hits (bank-conflict-free, clear_block_progression)
+      // small primes: a warp per prime
+      const uint32_t split = Lt / kSmallSplitDiv;
       const uint32_t lane_ofs = 4u * (uint32_t)lane;
       for (;;) {
         uint32_t i = 0;
@@ -549,13 +580,24 @@ sieve_tiles_kernel(SieveArgs a) {
         const uint32_t p = a.primes[i];
         const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
         const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
-        const uint32_t lp = lane_ofs * p;
-#pragma unroll 1
-        for (uint32_t o = 0; o < 8; ++o) {
+        if (p >= split) {
+          // 4 lanes per residue progression (lane = 4 o + q: bytes s_o + q p + 4p k)
+          const uint32_t o = (uint32_t)lane >> 2;
           const uint32_t e = s_step[bi * 8u + o];
           const uint32_t delta = pa * w30(o) + (e & 31u);
           const uint32_t s = delta >= r ? delta - r : delta + p - r;
-          clear_block_progression(bm, s + lp, p, e >> 5, Lt, nw, err);
+          clear_lane_progression(bm, s + ((uint32_t)lane & 3u) * p, p, e >> 5, Lt, nw, err);
+        } else {
+          // the eight residue progressions in turn, each split over all lanes in blocks of four
+          // consecutive hits (bank-conflict-free, clear_block_progression)
+          const uint32_t lp = lane_ofs * p;
+#pragma unroll 1
+          for (uint32_t o = 0; o < 8; ++o) {
+            const uint32_t e = s_step[bi * 8u + o];
+            const uint32_t delta = pa * w30(o) + (e & 31u);
+            const uint32_t s = delta >= r ? delta - r : delta + p - r;
+            clear_block_progression(bm, s + lp, p, e >> 5, Lt, nw, err);
+          }
         }
       }
       VOSS_PHASE(3)

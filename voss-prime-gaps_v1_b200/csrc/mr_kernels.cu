@@ -177,49 +177,6 @@ __device__ bool is_prime_u64_dev(uint64_t n) {
   return sprp_rest(M, d, r);
 }
 
-__global__ void mr_sieve_kernel(const uint64_t* __restrict__ cand, uint64_t count,
-                                uint8_t* __restrict__ out, uint32_t* __restrict__ work,
-                                uint32_t* __restrict__ nwork) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < count; base += stride) {
-    const uint64_t i = base + threadIdx.x;
-    bool need = false;
-    if (i < count) {
-      const uint64_t n = cand[i];
-      const int t = trial_phase(n);
-      if (t >= 0) {
-        out[i] = (uint8_t)t;
-      } else {
-        const Mont M = mont_setup(n);
-        uint64_t d = n - 1;
-        const int r = __ffsll((long long)d) - 1;
-        d >>= r;
-        if (!sprp2(M, d, r)) out[i] = 0;
-        else need = true;
-      }
-    }
-    __syncwarp();
-    // survivors below kSmallMr (6 bases) fill the work list from the front, the others from the
-    // back, so that the warps of mr_finish_kernel mostly share one base count
-    const bool small = need && cand[i] < kSmallMr;
-    const unsigned ms = __ballot_sync(0xFFFFFFFFu, small);
-    const unsigned ml = __ballot_sync(0xFFFFFFFFu, need && !small);
-    if (ms | ml) {
-      const int lane = threadIdx.x & 31;
-      uint32_t s0 = 0, s1 = 0;
-      if (lane == 0) {
-        if (ms) s0 = atomicAdd(nwork, (uint32_t)__popc(ms));
-        if (ml) s1 = atomicAdd(nwork + 1, (uint32_t)__popc(ml));
-      }
-      s0 = __shfl_sync(0xFFFFFFFFu, s0, 0);
-      s1 = __shfl_sync(0xFFFFFFFFu, s1, 0);
-      const unsigned below = (1u << lane) - 1u;
-      if (small) work[s0 + __popc(ms & below)] = (uint32_t)i;
-      else if (need) work[count - 1 - (s1 + __popc(ml & below))] = (uint32_t)i;
-    }
-  }
-}
-
 // Warp-uniform strong probable-prime test: every lane runs the same number of squarings and
 // multiplications (the warp's longest exponent and largest r) and keeps its verdict in a flag.
 // Early exits inside these loops let the lanes of a warp drift apart and never reconverge
@@ -295,6 +252,89 @@ __device__ __forceinline__ bool sprp_bases_3_on(const Mont& M, uint64_t d, int r
     prime = want ? pass : prime;
   }
   return prime;
+}
+
+// Trial division for every candidate (a lane per candidate), then base 2 for the undecided ones:
+// those wait in the warp's shared-memory queues, one for n below 3,474,749,660,383 (exponents of
+// at most 42 bits, six bases needed) and one for the rest, and each time a queue holds 32 they are
+// tested together with warp-uniform loops (sprp_uniform), a lane each.  Lanes whose candidate
+// trial division decides, and short exponents beside long ones, would otherwise leave most of the
+// warp idle (13 of 32 lanes active per instruction when each lane ran its own test).  Base-2
+// survivors go to the work list: the small ones from the front, the others from the back, so that
+// the warps of mr_finish_kernel mostly share one base count.
+constexpr int kSieveBlock = 256;
+constexpr int kMrQueue = 64;  // per warp and size class: at most 31 waiting + 32 arriving
+
+__device__ __forceinline__ void mr_base2_drain(const uint64_t* __restrict__ cand, uint8_t* __restrict__ out,
+                                               uint32_t* __restrict__ work, uint32_t* __restrict__ nwork,
+                                               uint64_t count, uint32_t* q, uint32_t& nq, bool small_class,
+                                               uint32_t lane) {
+  __syncwarp();
+  const uint32_t take = nq < 32u ? nq : 32u;
+  const bool live = lane < take;
+  uint32_t i = live ? q[lane] : 0u;
+  __syncwarp();
+  if (lane + 32u < nq) q[lane] = q[lane + 32u];
+  nq -= take;
+  __syncwarp();
+  const uint32_t i0 = __shfl_sync(0xFFFFFFFFu, i, 0);  // idle lanes shadow lane 0
+  if (!live) i = i0;
+  const uint64_t n = cand[i];
+  const Mont M = mont_setup(n);
+  uint64_t d = n - 1;
+  const int r = __ffsll((long long)d) - 1;
+  d >>= r;
+  const int top_w = __reduce_max_sync(0xFFFFFFFFu, (unsigned)(63 - __clzll(d)));
+  const int r_w = __reduce_max_sync(0xFFFFFFFFu, (unsigned)r);
+  const bool ok = __all_sync(0xFFFFFFFFu, n < (1ull << 63)) ? sprp_uniform<true>(M, 0, d, r, top_w, r_w, true)
+                                                           : sprp_uniform<false>(M, 0, d, r, top_w, r_w, true);
+  if (live && !ok) out[i] = 0;
+  const bool keep = live && ok;
+  const unsigned mk = __ballot_sync(0xFFFFFFFFu, keep);
+  if (mk) {
+    uint32_t at = 0;
+    if (lane == 0) at = atomicAdd(nwork + (small_class ? 0 : 1), (uint32_t)__popc(mk));
+    at = __shfl_sync(0xFFFFFFFFu, at, 0) + (uint32_t)__popc(mk & ((1u << lane) - 1u));
+    if (keep) {
+      if (small_class) work[at] = i;
+      else work[count - 1 - at] = i;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSieveBlock) mr_sieve_kernel(const uint64_t* __restrict__ cand, uint64_t count,
+                                                              uint8_t* __restrict__ out, uint32_t* __restrict__ work,
+                                                              uint32_t* __restrict__ nwork) {
+  __shared__ uint32_t s_q[kSieveBlock / 32][2][kMrQueue];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t* qs = s_q[warp][0];
+  uint32_t* ql = s_q[warp][1];
+  uint32_t ns = 0, nl = 0;  // warp-uniform queue lengths
+  const unsigned below = (1u << lane) - 1u;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + 32u * warp; base < count; base += stride) {
+    const uint64_t i = base + lane;
+    bool und = false, small = false;
+    if (i < count) {
+      const uint64_t n = cand[i];
+      const int t = trial_phase(n);
+      if (t >= 0) out[i] = (uint8_t)t;
+      else {
+        und = true;
+        small = n < kSmallMr;
+      }
+    }
+    const unsigned ms = __ballot_sync(0xFFFFFFFFu, und && small);
+    const unsigned ml = __ballot_sync(0xFFFFFFFFu, und && !small);
+    if (und && small) qs[ns + __popc(ms & below)] = (uint32_t)i;
+    if (und && !small) ql[nl + __popc(ml & below)] = (uint32_t)i;
+    ns += __popc(ms);
+    nl += __popc(ml);
+    if (ns >= 32u) mr_base2_drain(cand, out, work, nwork, count, qs, ns, true, lane);
+    if (nl >= 32u) mr_base2_drain(cand, out, work, nwork, count, ql, nl, false, lane);
+  }
+  if (ns) mr_base2_drain(cand, out, work, nwork, count, qs, ns, true, lane);
+  if (nl) mr_base2_drain(cand, out, work, nwork, count, ql, nl, false, lane);
 }
 
 // `work` holds candidate indices (< 2^32: the entry points take fewer than 2^32 candidates per call):
@@ -459,7 +499,7 @@ int launch_mr(const uint64_t* d_n, uint64_t count, uint8_t* d_out, uint32_t* d_w
   const int blk = 256;
   uint64_t want = (count + blk - 1) / blk;
   int grid = (int)(want < (uint64_t)sm_count * 16 ? want : (uint64_t)sm_count * 16);
-  mr_sieve_kernel<<<grid, blk, 0, s>>>(d_n, count, d_out, d_work, d_nwork);
+  mr_sieve_kernel<<<grid, kSieveBlock, 0, s>>>(d_n, count, d_out, d_work, d_nwork);
   mr_finish_kernel<<<sm_count * 8, blk, 0, s>>>(d_n, d_out, d_work, d_nwork, (uint32_t)count);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -976,38 +976,13 @@ int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_int
 // them in the launch's large-prime bitmap with global atomics.  The prime table is read once
 // per launch instead of once per tile, which is what bounds high intervals (at 1e18 the table
 // is 610 MB).  The tile kernel ANDs this bitmap into its fill and skips these primes.
-constexpr int kScatterChunk = 512;   // 20 KB of interval descriptors per block
-constexpr int kScatterQueue = 64;    // hits queued per warp (at most 31 + 32 between drains)
+constexpr int kScatterChunk = 960;  // 45 KB of interval descriptors per block
 
-// A (prime, interval) pair whose first coprime multiple lies inside the interval, waiting for a
-// lane to walk it.
-struct ScatterHit {
-  uint32_t gword;  // the interval's first word in the large-prime bitmap (< 2^32: checked on the host)
-  uint32_t lt;     // bytes of the interval's bitmap
-  uint32_t byte;   // byte of the first coprime multiple
-  uint32_t pa;     // p / 30
-  uint32_t bj;     // wheel class of p << 3 | wheel index of the first multiple's cofactor
-};
-
-// Walks the coprime multiples p*m of one queued hit through the interval's bitmap words.
-__device__ __forceinline__ void scatter_walk(const ScatterHit& h, const uint8_t* s_wstep, uint32_t* gbm) {
-  const uint8_t* row = s_wstep + (h.bj >> 3) * 8u;
-  uint32_t byte = h.byte, w = h.bj & 7u;
-  uint32_t* g = gbm + h.gword;
-  while (byte < h.lt) {
-    const uint32_t e = row[w];
-    atomicAnd(g + (byte >> 2), ~(1u << (((byte & 3u) << 3) | (e & 7u))));
-    byte += h.pa * ((e >> 5) & 6u) + ((e >> 3) & 7u);
-    w = (w + 1u) & 7u;
-  }
-}
-
-__global__ void __launch_bounds__(512, 4) scatter_large_kernel(const uint32_t* __restrict__ primes,
+__global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __restrict__ primes,
                                                             const uint64_t* __restrict__ magic, uint32_t j0,
                                                             uint32_t j1, const IntervalScatter* __restrict__ iv,
                                                             uint32_t n_iv, uint32_t* __restrict__ gbm) {
   __shared__ IntervalScatter s_iv[kScatterChunk];
-  __shared__ ScatterHit s_q[512 / 32][kScatterQueue];
   __shared__ int8_t s_rb[32];
   __shared__ uint8_t s_wstart[240];
   __shared__ uint8_t s_wstep[64];
@@ -1016,76 +991,54 @@ __global__ void __launch_bounds__(512, 4) scatter_large_kernel(const uint32_t* _
   if (threadIdx.x < 64) s_wstep[threadIdx.x] = c_walk_step[threadIdx.x];
   for (uint32_t i = threadIdx.x; i < n_iv; i += blockDim.x) s_iv[i] = iv[i];
   __syncthreads();
-  // A lane per prime tests the pairs; the pairs with a multiple inside (a minority, and their
-  // walks of very unequal length) go to the warp's queue and are walked 32 at a time, one per
-  // lane, so that the walks do not leave most of the warp idle.
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t below = (1u << lane) - 1u;
-  ScatterHit* q = s_q[warp];
-  uint32_t qn = 0;  // warp-uniform queue length
   const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t jw = j0 + blockIdx.x * blockDim.x + warp * 32u; jw < j1; jw += stride) {
-    const uint32_t j = jw + lane;
-    const bool valid = j < j1;
-    const uint32_t p = valid ? primes[j] : 0xFFFFFFFFu;  // >= 8 tile spans >= 2^11 (mod_by_estimate's range)
+  for (uint32_t j = j0 + blockIdx.x * blockDim.x + threadIdx.x; j < j1; j += stride) {
+    const uint32_t p = primes[j];  // >= 8 tile spans >= 2^11 (mod_by_estimate's range)
     const double inv = 1.0 / (double)p;
-    const uint32_t pa = p / 30u, bi = valid ? (uint32_t)s_rb[p - 30u * pa] : 0u;
+    const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
+    const uint8_t* row = s_wstep + bi * 8u;
     const bool narrow = p < (1u << 30);
     for (uint32_t s = 0; s < n_iv; ++s) {
       // vbase mod p from the truncated quotient estimate q (within one of floor(vbase / p), as in
       // mod_by_estimate): vbase - q p lies in (-p, 2p), inside the int32 range for p < 2^30, so
       // only the low 32 bits of vbase and of q p are needed (p >= 2^30, for hi above 2^60, takes
       // the 64-bit form)
+      const double vd = s_iv[s].vbase_d;
       const uint2 lo_sq = *reinterpret_cast<const uint2*>(&s_iv[s].vbase_lo);  // (vbase_lo, sqrt_hi)
-      const bool act = valid && p <= lo_sq.y;
-      if (!__any_sync(0xFFFFFFFFu, act)) break;  // intervals are sorted by sqrt_hi, descending
-      bool hit = false;
-      ScatterHit h;
-      if (act) {
-        const unsigned long long qt = __double2ull_rz(s_iv[s].vbase_d * inv);
-        int64_t rr;
-        if (narrow) rr = (int32_t)(lo_sq.x - (uint32_t)qt * p);
-        else rr = (int64_t)(s_iv[s].vbase - qt * (uint64_t)p);
-        rr += rr < 0 ? (int64_t)p : 0;
-        rr -= rr >= (int64_t)p ? (int64_t)p : 0;
-        const uint32_t d = rr ? p - (uint32_t)rr : 0u;  // first multiple of p, offset from vbase
-        const uint2 sp_lt = *reinterpret_cast<const uint2*>(&s_iv[s].span32);  // (span32, lt32)
-        if (d < sp_lt.x) {
-          const IntervalScatter& I = s_iv[s];
-          if (sp_lt.y) {
-            // the first multiple p*m with gcd(m, 30) = 1 (vbase is a multiple of 30)
-            const uint32_t st = s_wstart[bi * 30u + (d - 30u * (d / 30u))];
-            const uint64_t off = (uint64_t)d + (uint64_t)(st & 7u) * p;
-            if (off < I.span) {
-              hit = true;
-              h = ScatterHit{(uint32_t)I.gword, sp_lt.y, (uint32_t)(off / 30ull), pa, (bi << 3) | (st >> 3)};
-            }
-          } else {
-            // bitmaps of 2^31 bytes or more: every multiple, in 64-bit arithmetic, in place
-            for (uint64_t dd = d; dd < I.span; dd += p) {
-              const uint64_t q64 = dd / 30ull;
-              const int b = s_rb[(uint32_t)(dd - 30ull * q64)];
-              if (b >= 0) atomicAnd(gbm + I.gword + (q64 >> 2), ~(1u << ((((uint32_t)q64 & 3u) << 3) | (uint32_t)b)));
-            }
-          }
+      if (p > lo_sq.y) break;
+      const unsigned long long q = __double2ull_rz(vd * inv);
+      int64_t rr;
+      if (narrow) rr = (int32_t)(lo_sq.x - (uint32_t)q * p);
+      else rr = (int64_t)(s_iv[s].vbase - q * (uint64_t)p);
+      rr += rr < 0 ? (int64_t)p : 0;
+      rr -= rr >= (int64_t)p ? (int64_t)p : 0;
+      const uint32_t d = rr ? p - (uint32_t)rr : 0u;  // first multiple of p, offset from vbase
+      const uint2 sp_lt = *reinterpret_cast<const uint2*>(&s_iv[s].span32);  // (span32, lt32)
+      if (d >= sp_lt.x) continue;                      // none in the interval
+      const IntervalScatter& I = s_iv[s];
+      if (sp_lt.y) {
+        // wheel walk over the multiples p*m with gcd(m, 30) = 1 (vbase is a multiple of 30)
+        const uint32_t st = s_wstart[bi * 30u + (d - 30u * (d / 30u))];
+        const uint64_t off = (uint64_t)d + (uint64_t)(st & 7u) * p;
+        if (off >= I.span) continue;
+        uint32_t byte = (uint32_t)(off / 30ull), w = st >> 3;
+        const uint32_t lt = sp_lt.y;
+        uint32_t* g = gbm + I.gword;
+        while (byte < lt) {
+          const uint32_t e = row[w];
+          atomicAnd(g + (byte >> 2), ~(1u << (((byte & 3u) << 3) | (e & 7u))));
+          byte += pa * ((e >> 5) & 6u) + ((e >> 3) & 7u);
+          w = (w + 1u) & 7u;
         }
-      }
-      const uint32_t m = __ballot_sync(0xFFFFFFFFu, hit);
-      if (hit) q[qn + __popc(m & below)] = h;
-      qn += __popc(m);
-      if (qn >= 32u) {
-        __syncwarp();
-        const ScatterHit mine = q[lane];
-        __syncwarp();
-        if (lane < qn - 32u) q[lane] = q[32u + lane];
-        qn -= 32u;
-        __syncwarp();
-        scatter_walk(mine, s_wstep, gbm);
+      } else {
+        for (uint64_t dd = d; dd < I.span; dd += p) {
+          const uint64_t q64 = dd / 30ull;
+          const int b = s_rb[(uint32_t)(dd - 30ull * q64)];
+          if (b >= 0) atomicAnd(gbm + I.gword + (q64 >> 2), ~(1u << ((((uint32_t)q64 & 3u) << 3) | (uint32_t)b)));
+        }
       }
     }
   }
-  __syncwarp();
-  if (lane < qn) scatter_walk(q[lane], s_wstep, gbm);
 }
 
 int launch_scatter_large(const uint32_t* primes, const uint64_t* magic, uint32_t j0, uint32_t j1,

@@ -244,7 +244,6 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
                                  c->primes.begin());
   const size_t gbm_bytes = (size_t)P.n_words * 4;
   bool scatter = P.n_tiles && j1 > j0 && p_large <= 0xFFFFFFFFull && gbm_bytes <= W.gbm_budget &&
-                 P.n_words < (1ull << 32) &&  // word indices of the bitmap fit 32 bits
                  (!W.gbm_fixed || gbm_bytes <= W.gbm.bytes);
   std::vector<IntervalScatter> sc;
   // Windows of consecutive intervals whose bitmap words total at most kScatterWindowBytes: the

@@ -978,62 +978,6 @@ int launch_interval_finalize(const SieveArgs& a, const IntervalOut* io, voss_int
 // is 610 MB).  The tile kernel ANDs this bitmap into its fill and skips these primes.
 constexpr int kScatterChunk = 960;  // 45 KB of interval descriptors per block
 
-// All (p, interval) pairs of one prime p: the remainder of each interval's start, then, when a
-// multiple of p falls inside, a wheel walk over the multiples coprime to 30.  kNarrow (p < 2^30):
-// vbase - q p, q the truncated quotient estimate (within one of floor(vbase / p), as in
-// mod_by_estimate), lies in (-p, 2p), inside the int32 range, so the remainder needs only the
-// low 32 bits of vbase and of q p and stays in 32-bit arithmetic; primes of 2^30 and more (hi
-// above 2^60) take the 64-bit form.
-template <bool kNarrow>
-__device__ __forceinline__ void scatter_prime(uint32_t p, const IntervalScatter* s_iv, uint32_t n_iv,
-                                              const int8_t* s_rb, const uint8_t* s_wstart, const uint8_t* s_wstep,
-                                              uint32_t* __restrict__ gbm) {
-  const double inv = 1.0 / (double)p;
-  const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
-  const uint8_t* row = s_wstep + bi * 8u;
-  for (uint32_t s = 0; s < n_iv; ++s) {
-    const uint2 lo_sq = *reinterpret_cast<const uint2*>(&s_iv[s].vbase_lo);  // (vbase_lo, sqrt_hi)
-    if (p > lo_sq.y) break;  // intervals are sorted by sqrt_hi, descending
-    const double vd = s_iv[s].vbase_d;
-    uint32_t d;  // first multiple of p, offset from vbase
-    if (kNarrow) {
-      uint32_t r = lo_sq.x - (uint32_t)__double2ull_rz(vd * inv) * p;
-      r += (int32_t)r < 0 ? p : 0u;
-      r -= r >= p ? p : 0u;
-      d = r ? p - r : 0u;
-    } else {
-      int64_t rr = (int64_t)(s_iv[s].vbase - __double2ull_rz(vd * inv) * (uint64_t)p);
-      rr += rr < 0 ? (int64_t)p : 0;
-      rr -= rr >= (int64_t)p ? (int64_t)p : 0;
-      d = rr ? p - (uint32_t)rr : 0u;
-    }
-    const uint2 sp_lt = *reinterpret_cast<const uint2*>(&s_iv[s].span32);  // (span32, lt32)
-    if (d >= sp_lt.x) continue;                      // none in the interval
-    const IntervalScatter& I = s_iv[s];
-    if (sp_lt.y) {
-      // wheel walk over the multiples p*m with gcd(m, 30) = 1 (vbase is a multiple of 30)
-      const uint32_t st = s_wstart[bi * 30u + (d - 30u * (d / 30u))];
-      const uint64_t off = (uint64_t)d + (uint64_t)(st & 7u) * p;
-      if (off >= I.span) continue;
-      uint32_t byte = (uint32_t)(off / 30ull), w = st >> 3;
-      const uint32_t lt = sp_lt.y;
-      uint32_t* g = gbm + I.gword;
-      while (byte < lt) {
-        const uint32_t e = row[w];
-        atomicAnd(g + (byte >> 2), ~(1u << (((byte & 3u) << 3) | (e & 7u))));
-        byte += pa * ((e >> 5) & 6u) + ((e >> 3) & 7u);
-        w = (w + 1u) & 7u;
-      }
-    } else {
-      for (uint64_t dd = d; dd < I.span; dd += p) {
-        const uint64_t q64 = dd / 30ull;
-        const int b = s_rb[(uint32_t)(dd - 30ull * q64)];
-        if (b >= 0) atomicAnd(gbm + I.gword + (q64 >> 2), ~(1u << ((((uint32_t)q64 & 3u) << 3) | (uint32_t)b)));
-      }
-    }
-  }
-}
-
 __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __restrict__ primes,
                                                             const uint64_t* __restrict__ magic, uint32_t j0,
                                                             uint32_t j1, const IntervalScatter* __restrict__ iv,
@@ -1050,8 +994,50 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t j = j0 + blockIdx.x * blockDim.x + threadIdx.x; j < j1; j += stride) {
     const uint32_t p = primes[j];  // >= 8 tile spans >= 2^11 (mod_by_estimate's range)
-    if (p < (1u << 30)) scatter_prime<true>(p, s_iv, n_iv, s_rb, s_wstart, s_wstep, gbm);
-    else scatter_prime<false>(p, s_iv, n_iv, s_rb, s_wstart, s_wstep, gbm);
+    const double inv = 1.0 / (double)p;
+    const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
+    const uint8_t* row = s_wstep + bi * 8u;
+    const bool narrow = p < (1u << 30);
+    for (uint32_t s = 0; s < n_iv; ++s) {
+      // vbase mod p from the truncated quotient estimate q (within one of floor(vbase / p), as in
+      // mod_by_estimate): vbase - q p lies in (-p, 2p), inside the int32 range for p < 2^30, so
+      // only the low 32 bits of vbase and of q p are needed (p >= 2^30, for hi above 2^60, takes
+      // the 64-bit form)
+      const double vd = s_iv[s].vbase_d;
+      const uint2 lo_sq = *reinterpret_cast<const uint2*>(&s_iv[s].vbase_lo);  // (vbase_lo, sqrt_hi)
+      if (p > lo_sq.y) break;
+      const unsigned long long q = __double2ull_rz(vd * inv);
+      int64_t rr;
+      if (narrow) rr = (int32_t)(lo_sq.x - (uint32_t)q * p);
+      else rr = (int64_t)(s_iv[s].vbase - q * (uint64_t)p);
+      rr += rr < 0 ? (int64_t)p : 0;
+      rr -= rr >= (int64_t)p ? (int64_t)p : 0;
+      const uint32_t d = rr ? p - (uint32_t)rr : 0u;  // first multiple of p, offset from vbase
+      const uint2 sp_lt = *reinterpret_cast<const uint2*>(&s_iv[s].span32);  // (span32, lt32)
+      if (d >= sp_lt.x) continue;                      // none in the interval
+      const IntervalScatter& I = s_iv[s];
+      if (sp_lt.y) {
+        // wheel walk over the multiples p*m with gcd(m, 30) = 1 (vbase is a multiple of 30)
+        const uint32_t st = s_wstart[bi * 30u + (d - 30u * (d / 30u))];
+        const uint64_t off = (uint64_t)d + (uint64_t)(st & 7u) * p;
+        if (off >= I.span) continue;
+        uint32_t byte = (uint32_t)(off / 30ull), w = st >> 3;
+        const uint32_t lt = sp_lt.y;
+        uint32_t* g = gbm + I.gword;
+        while (byte < lt) {
+          const uint32_t e = row[w];
+          atomicAnd(g + (byte >> 2), ~(1u << (((byte & 3u) << 3) | (e & 7u))));
+          byte += pa * ((e >> 5) & 6u) + ((e >> 3) & 7u);
+          w = (w + 1u) & 7u;
+        }
+      } else {
+        for (uint64_t dd = d; dd < I.span; dd += p) {
+          const uint64_t q64 = dd / 30ull;
+          const int b = s_rb[(uint32_t)(dd - 30ull * q64)];
+          if (b >= 0) atomicAnd(gbm + I.gword + (q64 >> 2), ~(1u << ((((uint32_t)q64 & 3u) << 3) | (uint32_t)b)));
+        }
+      }
+    }
   }
 }
 

@@ -422,6 +422,8 @@ sieve_tiles_kernel(SieveArgs a) {
   __shared__ uint32_t s_pos[32];  // bit b of a word -> integer offset 30 * (b / 8) + W30[b % 8]
   __shared__ uint8_t s_wstart[240];
   __shared__ uint8_t s_wstep[64];
+  __shared__ uint32_t s_rank[EMIT ? 1 : BLOCK];   // first tile rank of each thread's chunk
+  __shared__ int32_t s_before[EMIT ? 1 : BLOCK];  // last prime before each chunk (-1: none)
   uint32_t* err = a.error;
 
   const int tid = threadIdx.x, lane = tid & 31;
@@ -716,52 +718,79 @@ sieve_tiles_kernel(SieveArgs a) {
       }
       __syncthreads();
     } else {
-      // pass 1: last prime of my chunk
+      // pass 1: the primes of my chunk and its last prime
+      uint32_t pc = 0;
       int32_t my_last = -1;
-      for (uint32_t w = cend; w > c0;) {
-        --w;
+      for (uint32_t w = c0; w < cend; ++w) {
         const uint32_t x = bm[w];
-        if (x) {
-          const uint32_t b = 31u - (uint32_t)__clz(x);
-          my_last = (int32_t)(120u * w + 30u * (b >> 3) + w30(b & 7u));
-          break;
-        }
+        pc += (uint32_t)__popc(x);
+        if (x) my_last = (int32_t)(120u * w + s_pos[31u - (uint32_t)__clz(x)]);
       }
+      uint32_t tile_cnt;
+      const uint32_t rank0 = block_excl_sum<BLOCK>(pc, S, &tile_cnt);
       int32_t tile_last;
-      int32_t prev = block_excl_max<BLOCK>(my_last, S, &tile_last);
+      const int32_t before = block_excl_max<BLOCK>(my_last, S, &tile_last);
+      s_rank[tid] = rank0;
+      s_before[tid] = before;
+      __syncthreads();
       VOSS_PHASE(7)
 
-      // pass 2: walk the chunk in order.  The class counters of a word's 4 bytes are indexed
-      // without wrapping (k mod 28 + j up to 30, k mod 143 + j up to 145: 31 and 146 classes);
-      // the flush folds the tail classes back.  That makes both class indices one add per prime.
+      // pass 2: every thread walks the same number of the tile's primes in order (ranks
+      // [ra, rb) of tile_cnt), so that the lanes of a warp run the same trip count.  The start
+      // is the prime of rank ra: the chunk holding it is the last one whose first rank is <= ra.
+      const uint32_t ra = (uint32_t)(((unsigned long long)tile_cnt * (uint32_t)tid) / BLOCK);
+      const uint32_t rb = (uint32_t)(((unsigned long long)tile_cnt * ((uint32_t)tid + 1u)) / BLOCK);
+      const uint32_t n_mine = rb - ra;
+      uint32_t w = 0, x = 0;
+      int32_t prev = -1;
+      if (n_mine) {
+        uint32_t lo = 0, hi = BLOCK;  // s_rank[lo] <= ra
+        while (hi - lo > 1u) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (s_rank[mid] <= ra) lo = mid; else hi = mid;
+        }
+        uint32_t k = ra - s_rank[lo];
+        prev = s_before[lo];
+        w = lo * C;
+        x = bm[w];
+        for (;;) {  // the word holding the start: it lies in chunk lo
+          const uint32_t c = (uint32_t)__popc(x);
+          if (k < c) break;
+          if (x) prev = (int32_t)(120u * w + s_pos[31u - (uint32_t)__clz(x)]);
+          k -= c;
+          x = bm[++w];
+        }
+        for (; k; --k) {  // the primes of that word before mine
+          prev = (int32_t)(120u * w + s_pos[(uint32_t)__ffs(x) - 1u]);
+          x &= x - 1u;
+        }
+      }
+      // The class counters of a word's 4 bytes are indexed without wrapping (k mod 28 + j up to
+      // 30, k mod 143 + j up to 145: 31 and 146 classes); the flush folds the tail classes back.
+      // That makes both class indices one add per prime.
       const uint32_t vb = H.vb;
       const uint32_t cthr = H.cthr;
-      uint32_t c28 = (uint32_t)kSmCls28 + 8u * ((H.k28 + 4u * c0) % 28u);
-      uint32_t c143 = (uint32_t)kSmCls143 + 8u * ((H.k143 + 4u * c0) % 143u);
-      uint32_t my_cnt = 0, mg = 0, mlo = 0;
+      uint32_t c28 = (uint32_t)kSmCls28 + 8u * ((H.k28 + 4u * w) % 28u);
+      uint32_t c143 = (uint32_t)kSmCls143 + 8u * ((H.k143 + 4u * w) % 143u);
+      uint32_t mg = 0, mlo = 0;
       uint32_t mq_prev = 0;  // modq row of the previous prime
       if (prev >= 0) {
         const uint32_t kp = (uint32_t)prev / 30u;
         mq_prev = (uint32_t)kSmModq + kModqBins * (uint32_t)s_rb[(uint32_t)prev - 30u * kp];
       }
-      uint32_t w = c0;
-      uint32_t x = w < cend ? bm[w] : 0u;
       uint32_t wpos = 120u * w;
-      for (;;) {
-        while (x == 0u) {
-          if (++w >= cend) break;
-          x = bm[w];
+      for (uint32_t it = 0; it < n_mine; ++it) {
+        while (x == 0u) {  // the tile holds rb >= ra + it + 1 primes: w stays inside it
+          x = bm[++w];
           wpos += 120u;
           c28 += 32u;
           if (c28 >= (uint32_t)kSmCls28 + 224u) c28 -= 224u;
           c143 += 32u;
           if (c143 >= (uint32_t)kSmCls143 + 1144u) c143 -= 1144u;
         }
-        if (w >= cend) break;
         const uint32_t b = (uint32_t)__ffs(x) - 1u;
         x &= x - 1u;
         const uint32_t pos = wpos + s_pos[b];
-        ++my_cnt;
         sm_add(cnt, c28 + b, err);
         sm_add(cnt, c143 + b, err);
         const uint32_t mq = (uint32_t)kSmModq + kModqBins * (b & 7u);
@@ -798,11 +827,12 @@ sieve_tiles_kernel(SieveArgs a) {
       }
       const unsigned long long key =
           mg ? (((unsigned long long)mg << 32) | (unsigned long long)(0xFFFFFFFFu - mlo)) : 0ull;
-      uint32_t tile_cnt;
+      uint32_t tile_cnt2;
       unsigned long long tile_key;
       __syncthreads();  // H.first visible, scratch reuse
       VOSS_PHASE(8)
-      block_reduce_tile<BLOCK>(my_cnt, key, S, &tile_cnt, &tile_key);
+      block_reduce_tile<BLOCK>(n_mine, key, S, &tile_cnt2, &tile_key);
+      (void)tile_cnt2;  // = tile_cnt
       if (tid == 0) {
         TilePartial P;
         P.first = tile_cnt ? H.first : kNone;

@@ -274,6 +274,7 @@ struct TileHdr {
   uint32_t pre_base[kPreGroups];
   uint32_t interval, tile, next_tile, cur_iv, since_flush, flush;
   uint32_t r0, r1;       // base primes lying in the tile (restore)
+  uint32_t c_lt, c_np, c_ia, c_ib, c_iw;  // category bounds of the CTA's last (tile length, np)
   uint32_t coop_ctr, b_ctr, c_ctr;  // work counters of the three prime categories
   unsigned long long gword;         // the tile's first word in the large-prime bitmap
   uint32_t first;
@@ -440,6 +441,8 @@ sieve_tiles_kernel(SieveArgs a) {
     H.cur_iv = kNone;
     H.since_flush = 0;
     H.count_total = 0;
+    H.c_lt = kNone;
+    H.c_np = kNone;
   }
   __syncthreads();
 
@@ -497,18 +500,33 @@ sieve_tiles_kernel(SieveArgs a) {
       H.lt = 4u * nw;
       uint64_t vend = H.vbase + 30ull * H.lt;
       if (vend > iv.hi) vend = iv.hi;
-      uint32_t np = count_le(a.primes, a.n_primes, isqrt_u64(vend - 1));
+      // table searches, skipped where the answer is known: a tile past the table's last prime
+      // needs every prime and holds none of them, and the category bounds depend only on the
+      // tile length and np, so they are kept from the CTA's previous tile when those repeat
+      const uint64_t sq = isqrt_u64(vend - 1);
+      uint32_t np = sq >= a.p_max ? a.n_primes : count_le(a.primes, a.n_primes, sq);
       if (a.gbm && np > a.scatter_first) np = a.scatter_first;  // the rest came from the pre-pass
       H.np = np;
       H.gword = iv.gword + wofs;
-      uint32_t ia = count_lt(a.primes, np, (uint64_t)(H.lt / a.coop_div));
-      uint32_t ib = count_lt(a.primes, np, (uint64_t)H.lt * a.mult_factor);
-      H.ia = ia;
-      H.ib = ib < ia ? ia : ib;
-      const uint32_t iw = count_lt(a.primes, np, ((uint64_t)H.lt * a.walk_sixteenths) >> 4);
-      H.iw = iw < H.ia ? H.ia : (iw > H.ib ? H.ib : iw);
-      H.r0 = count_lt(a.primes, a.n_primes, H.vbase);
-      H.r1 = count_lt(a.primes, a.n_primes, H.vbase + 30ull * H.lt);
+      if (H.lt != H.c_lt || np != H.c_np) {
+        const uint32_t ia = count_lt(a.primes, np, (uint64_t)(H.lt / a.coop_div));
+        const uint32_t ib = count_lt(a.primes, np, (uint64_t)H.lt * a.mult_factor);
+        const uint32_t iw = count_lt(a.primes, np, ((uint64_t)H.lt * a.walk_sixteenths) >> 4);
+        H.c_ia = ia;
+        H.c_ib = ib < ia ? ia : ib;
+        H.c_iw = iw < H.c_ia ? H.c_ia : (iw > H.c_ib ? H.c_ib : iw);
+        H.c_lt = H.lt;
+        H.c_np = np;
+      }
+      H.ia = H.c_ia;
+      H.ib = H.c_ib;
+      H.iw = H.c_iw;
+      if (H.vbase > a.p_max) {
+        H.r0 = H.r1 = a.n_primes;
+      } else {
+        H.r0 = count_lt(a.primes, a.n_primes, H.vbase);
+        H.r1 = count_lt(a.primes, a.n_primes, H.vbase + 30ull * H.lt);
+      }
       uint32_t vb = kNone;
       if (iv.seg_k) {
         uint64_t kb = (ktile / iv.seg_k + 1) * iv.seg_k;

@@ -199,6 +199,7 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
   a.primes = c->d_primes.as<uint32_t>();
   a.magic = c->d_magic.as<uint64_t>();
   a.n_primes = (uint32_t)c->primes.size();
+  a.p_max = c->primes.empty() ? 0u : c->primes.back();
   a.pretab = c->d_pretab.as<uint32_t>();
   a.iv = W.iv.as<IntervalDev>();
   a.n_intervals = n_iv;

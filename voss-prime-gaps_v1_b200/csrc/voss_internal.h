@@ -128,6 +128,7 @@ struct SieveArgs {
   const uint32_t* primes;   // base primes >= 37, ascending
   const uint64_t* magic;    // floor((2^64-1)/p) per prime
   uint32_t n_primes;
+  uint32_t p_max;           // the last (largest) base prime, 0 when there is none
   const uint32_t* pretab;   // kPreWords presieve masks
   const IntervalDev* iv;
   uint32_t n_intervals;

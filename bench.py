@@ -207,7 +207,7 @@ def primes_upto(s: int):
     return p[p >= 7].astype(np.float64)
 
 
-def interval_work(lo, hi, p_large: int) -> dict:
+def interval_work(lo, hi, p_large: int, mr_route: int = 50) -> dict:
     """Algorithmic work terms of a batch of intervals [lo_i, hi_i).
 
     offsets: one first-hit computation per (interval, base prime 7 <= p <= isqrt(hi_i - 1)).
@@ -240,9 +240,25 @@ def interval_work(lo, hi, p_large: int) -> dict:
             sel = big[(big >= cuts[c]) & (big < cuts[c + 1])]
             if sel.size:
                 hits[c] += float(((b - sel * sel) / sel).sum())
+    # (prime, interval) pairs of the large-prime pre-pass: primes p_large <= p <= isqrt(hi - 1) of
+    # every interval the library sieves (those with more such primes than mr_route times their
+    # length go to Miller-Rabin instead, the rule of voss_sieve_intervals)
+    n_large_lt = int(np.searchsorted(P, float(p_large), side="left"))
+    pairs = routed = 0
+    for a, b in zip(lo.tolist(), hi.tolist()):
+        a7 = max(a, 7)
+        if b <= a7:
+            continue
+        np_hi = int(np.searchsorted(P, math.isqrt(b - 1), side="right"))
+        cnt = max(0, np_hi - n_large_lt)
+        if mr_route != 0xFFFFFFFF and b - a7 < (1 << 31) and cnt // mr_route > b - a7:
+            routed += 1
+            continue
+        pairs += cnt
     k = 8.0 / 30.0
     return {"first_hit_offsets": int(offsets), "presieve_primes_hits": k * hits[0],
             "tile_hits": k * hits[1], "prepass_hits": k * hits[2], "p_large": int(p_large),
+            "prepass_pairs": int(pairs), "mr_routed_intervals": int(routed),
             "note": "hits are expected counts, 8(hi - max(lo, p^2))/(30p) per (interval, prime)"}
 
 
@@ -418,7 +434,7 @@ def run_intervals(a) -> dict:
     pre_ms, tile_ms, tail_ms = (statistics.mean(ph[k] for ph in phases) for k in range(3))
     t = ctx.tuning()
     tile_bytes = 4 * t["block_threads"] * t["chunk_words"]
-    work = interval_work(lo, hi, t["mult_factor"] * tile_bytes)
+    work = interval_work(lo, hi, t["mult_factor"] * tile_bytes, t["mr_route"])
     smem_peak = ctx.probe_smem_rmw()
     # tile kernel: 8 B per shared-memory bit-clear + one read of the intervals' bitmap words
     alg_bytes = 8.0 * work["tile_hits"] + total_int / 30.0
@@ -437,6 +453,14 @@ def run_intervals(a) -> dict:
         "phases_ms": {"copies_memsets_prepass": pre_ms, "tile_kernel": tile_ms, "stitch_reduce_finalize": tail_ms},
         "work_terms": work,
         "prepass_clears_per_s": work["prepass_hits"] / (pre_ms * 1e-3) if pre_ms > 0 else None,
+        "prepass": {
+            "bound": "int", "pairs": work["prepass_pairs"],
+            "pairs_per_s": work["prepass_pairs"] / (pre_ms * 1e-3) if pre_ms > 0 else None,
+            "ms": pre_ms, "clears": work["prepass_hits"],
+            "issue_frac_ncu": 0.722, "alu_frac_ncu": 0.587,
+            "source": "issue and ALU-pipe fractions of peak (active cycles) of scatter_large_kernel from the "
+                      "committed capture profiles/scatter_large_kernel_intervals.md; one 64-bit reduction per "
+                      "(prime, interval) pair, ms includes the batch's copies and bitmap memset"},
         "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
                      "frac": achieved / smem_peak, "traffic": None, "kernel": "sieve_tiles_kernel",
                      "kernel_ms": tile_ms, "algorithmic_bytes": alg_bytes,

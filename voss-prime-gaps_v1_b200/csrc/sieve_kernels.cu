@@ -105,6 +105,7 @@ __device__ __forceinline__ uint32_t count_lt(const uint32_t* pr, uint32_t n, uin
 }
 
 __device__ __forceinline__ uint32_t find_interval(const SieveArgs& a, uint32_t t) {
+  if (a.tile_iv) return a.tile_iv[t];  // the launch's tile -> interval table
   uint32_t lo = 0, hi = a.n_intervals;  // largest i with tile_begin <= t
   while (hi - lo > 1) {
     uint32_t mid = (lo + hi) >> 1;
@@ -535,10 +536,11 @@ sieve_tiles_kernel(SieveArgs a) {
       H.vb = vb;
       // large-gap candidates: g >= cthr, one tile-uniform threshold.  Reference rule
       // (voss_v7_live.cu:289-294): g > 100 and (g >= 500 or g / log(p) >= 10); no gap of the tile
-      // below 10 log(vbase) - 2 can reach merit 10.  With large_min_gap: g >= large_min_gap.
-      double lv = log((double)(H.vbase > 7 ? H.vbase : 7));
-      double th = floor(10.0 * lv) - 2.0;
-      uint32_t gthr = th < 0 ? 0u : (th > 1e9 ? 1000000000u : (uint32_t)th);
+      // below 10 log(vbase) - 3 can reach merit 10.  With large_min_gap: g >= large_min_gap.
+      // (single-precision log: its error, a few units of 1e-6 relative at these sizes, is far
+      // inside the margin of 3; the kept gaps are then decided by the double merit below)
+      const float th = floorf(10.0f * __logf((float)(H.vbase > 7 ? H.vbase : 7))) - 3.0f;
+      uint32_t gthr = th < 0.0f ? 0u : (uint32_t)th;
       gthr = gthr < 101u ? 101u : (gthr > 500u ? 500u : gthr);
       H.cthr = !a.want_large ? kNone : (a.large_min_gap ? a.large_min_gap : gthr);
       H.k28 = (uint32_t)(ktile % 28ull);

@@ -287,10 +287,22 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
     a.gbm = W.gbm.as<uint32_t>();
     a.scatter_first = j0;
   }
+  // Tiles of a launch of many intervals find their interval in a table (one load) rather than
+  // by a binary search of the interval descriptors in the tile header.
+  std::vector<uint32_t> tiv;
+  if (n_iv > 1 && P.n_tiles) {
+    tiv.resize(P.n_tiles);
+    for (uint32_t i = 0; i < n_iv; ++i)
+      for (uint32_t t = 0; t < P.iv[i].n_tiles; ++t) tiv[P.iv[i].tile_begin + t] = i;
+    if ((rc = W.tile_iv.ensure(sizeof(uint32_t) * P.n_tiles))) return rc;
+    a.tile_iv = W.tile_iv.as<uint32_t>();
+  }
   // Device work of the launch, all of it after ev0 (the host planning above is done first, so
   // the GPU never waits on the host inside the events).
   CUDA_TRY(cudaEventRecord(E.ev0, s));
   if (n_iv) CUDA_TRY(cudaMemcpyAsync(W.iv.p, P.iv.data(), sizeof(IntervalDev) * n_iv, cudaMemcpyHostToDevice, s));
+  if (!tiv.empty())
+    CUDA_TRY(cudaMemcpyAsync(W.tile_iv.p, tiv.data(), sizeof(uint32_t) * tiv.size(), cudaMemcpyHostToDevice, s));
   if (!emit) CUDA_TRY(cudaMemsetAsync(W.acc.p, 0, sizeof(unsigned long long) * kAccStride * std::max<size_t>(1, n_iv), s));
   CUDA_TRY(cudaMemsetAsync(W.counters.p, 0, sizeof(uint32_t) * kCtrWords, s));
   if (scatter) {

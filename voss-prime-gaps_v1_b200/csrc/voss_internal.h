@@ -131,6 +131,7 @@ struct SieveArgs {
   uint32_t p_max;           // the last (largest) base prime, 0 when there is none
   const uint32_t* pretab;   // kPreWords presieve masks
   const IntervalDev* iv;
+  const uint32_t* tile_iv;  // interval of each tile (nullptr: found by binary search over iv)
   uint32_t n_intervals;
   uint32_t n_tiles;
   uint32_t tile_words;

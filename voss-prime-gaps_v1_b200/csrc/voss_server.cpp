@@ -293,6 +293,7 @@ Slot* make_slot(voss_server* S, int* rc) {
   Workspace& W = sl->ws;
   int e;
   if ((e = W.iv.ensure(sizeof(voss::IntervalDev) * nreq)) || (e = W.partials.ensure(sizeof(voss::TilePartial) * C.max_batch_tiles)) ||
+      (e = W.tile_iv.ensure(sizeof(uint32_t) * C.max_batch_tiles)) ||
       (e = W.acc.ensure(sizeof(unsigned long long) * voss::kAccStride * nreq)) ||
       (e = W.out.ensure(sizeof(IntervalOut) * nreq)) || (e = W.counters.ensure(sizeof(uint32_t) * kCtrWords)) ||
       (e = W.over.ensure(sizeof(voss::OverflowGap) * kOverCap)) || (e = W.large.ensure(sizeof(voss::LargeGapDev))) ||

@@ -119,7 +119,7 @@ int apply_tuning(voss_ctx* c, const voss_tuning& t0) {
   voss_tuning t = t0;
   if (!t.block_threads) t.block_threads = 1024;
   if (!t.chunk_words) t.chunk_words = t.block_threads == 1024 ? 49 : 45;
-  if (!t.coop_div) t.coop_div = 128;
+  if (!t.coop_div) t.coop_div = 80;
   if (!t.mult_factor) t.mult_factor = 8;
   if (!t.walk_sixteenths) t.walk_sixteenths = 4;
   if (!t.mr_route) t.mr_route = 50;

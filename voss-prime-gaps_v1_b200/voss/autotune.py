@@ -17,7 +17,7 @@ import numpy as np
 # candidate tunings: tile bytes from 200 KB (1 CTA/SM) down to 36 KB (several CTAs/SM), with the
 # small/medium split (coop_div) and the pre-pass threshold (mult_factor) near their measured optima
 CANDIDATES = [
-    dict(block_threads=1024, chunk_words=49, coop_div=128, mult_factor=8),
+    dict(block_threads=1024, chunk_words=49, coop_div=80, mult_factor=8),
     dict(block_threads=1024, chunk_words=49, coop_div=64, mult_factor=8),
     dict(block_threads=1024, chunk_words=49, coop_div=64, mult_factor=16),
     dict(block_threads=1024, chunk_words=25, coop_div=64, mult_factor=8),

@@ -189,21 +189,25 @@ __device__ __forceinline__ void clear_block_progression(uint32_t* bm, uint32_t b
 __device__ __forceinline__ void clear_progression(uint32_t* bm, uint32_t byte, uint32_t p, uint32_t bit,
                                                   uint32_t Lt, uint32_t nw, uint32_t* err) {
   if (byte + 3u * p < Lt) {
-    const uint32_t b1 = byte + p, b2 = b1 + p, b3 = b2 + p;
-    const uint32_t m0 = ~(1u << (((byte & 3u) << 3) | bit)), m1 = ~(1u << (((b1 & 3u) << 3) | bit));
-    const uint32_t m2 = ~(1u << (((b2 & 3u) << 3) | bit)), m3 = ~(1u << (((b3 & 3u) << 3) | bit));
+    // the four hits' byte lanes are j0, j0 + p, j0 + 2p, j0 + 3p (mod 4): one lane up each time
+    // for p = 1 (mod 4), one lane down for p = 3, so each mask is the previous one rotated by a byte
+    const uint32_t j0 = byte & 3u;
+    const uint32_t M0 = 1u << ((j0 << 3) | bit);
+    const uint32_t rot = (p & 2u) ? 24u : 8u;
+    const uint32_t M1 = __funnelshift_l(M0, M0, rot), M2 = __funnelshift_l(M1, M1, rot),
+                   M3 = __funnelshift_l(M2, M2, rot);
+    const uint32_t m0 = ~M0, m1 = ~M1, m2 = ~M2, m3 = ~M3;
     uint32_t w0 = byte >> 2;
-    const uint32_t d1 = (b1 >> 2) - w0, d2 = (b2 >> 2) - w0, d3 = (b3 >> 2) - w0;
+    const uint32_t d1 = (j0 + p) >> 2, d2 = (j0 + 2u * p) >> 2, d3 = (j0 + 3u * p) >> 2;
     // b3 + 4pk < Lt  <=>  w0 + k < lim  (w0 + d3 = b3 >> 2)
-    const uint32_t lim = ((Lt + 3u - (b3 & 3u)) >> 2) - d3;
-    uint32_t k = 0;
-    for (; w0 < lim; w0 += p, ++k) {
+    const uint32_t lim = ((Lt + 3u - ((j0 + 3u * p) & 3u)) >> 2) - d3;
+    for (; w0 < lim; w0 += p) {
       clear_bit_word(bm, w0, m0, nw, err);
       clear_bit_word(bm, w0 + d1, m1, nw, err);
       clear_bit_word(bm, w0 + d2, m2, nw, err);
       clear_bit_word(bm, w0 + d3, m3, nw, err);
     }
-    byte += 4u * p * k;
+    byte = (w0 << 2) | j0;  // the loop advanced by 4p bytes (p words) per trip
   }
   for (; byte < Lt; byte += p) clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
 }

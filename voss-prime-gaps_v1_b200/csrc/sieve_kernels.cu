@@ -1061,12 +1061,18 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
       const uint2 lo_sq = *reinterpret_cast<const uint2*>(&s_iv[s].vbase_lo);  // (vbase_lo, sqrt_hi)
       if (p > lo_sq.y) break;
       const unsigned long long q = __double2ull_rz(vd * inv);
-      int64_t rr;
-      if (narrow) rr = (int32_t)(lo_sq.x - (uint32_t)q * p);
-      else rr = (int64_t)(s_iv[s].vbase - q * (uint64_t)p);
-      rr += rr < 0 ? (int64_t)p : 0;
-      rr -= rr >= (int64_t)p ? (int64_t)p : 0;
-      const uint32_t d = rr ? p - (uint32_t)rr : 0u;  // first multiple of p, offset from vbase
+      uint32_t d;  // first multiple of p, offset from vbase
+      if (narrow) {  // 32-bit arithmetic: r = vbase - q p as int32 in (-p, 2p)
+        uint32_t r = lo_sq.x - (uint32_t)q * p;
+        r += (int32_t)r < 0 ? p : 0u;
+        r -= r >= p ? p : 0u;
+        d = r ? p - r : 0u;
+      } else {
+        int64_t rr = (int64_t)(s_iv[s].vbase - q * (uint64_t)p);
+        rr += rr < 0 ? (int64_t)p : 0;
+        rr -= rr >= (int64_t)p ? (int64_t)p : 0;
+        d = rr ? p - (uint32_t)rr : 0u;
+      }
       const uint2 sp_lt = *reinterpret_cast<const uint2*>(&s_iv[s].span32);  // (span32, lt32)
       if (d >= sp_lt.x) continue;                      // none in the interval
       const IntervalScatter& I = s_iv[s];

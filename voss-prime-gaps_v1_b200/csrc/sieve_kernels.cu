@@ -1052,18 +1052,21 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
     const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
     const uint8_t* row = s_wstep + bi * 8u;
     const bool narrow = p < (1u << 30);
-    for (uint32_t s = 0; s < n_iv; ++s) {
-      // vbase mod p from the truncated quotient estimate q (within one of floor(vbase / p), as in
-      // mod_by_estimate): vbase - q p lies in (-p, 2p), inside the int32 range for p < 2^30, so
-      // only the low 32 bits of vbase and of q p are needed (p >= 2^30, for hi above 2^60, takes
-      // the 64-bit form)
-      const double vd = s_iv[s].vbase_d;
-      const uint2 lo_sq = *reinterpret_cast<const uint2*>(&s_iv[s].vbase_lo);  // (vbase_lo, sqrt_hi)
-      if (p > lo_sq.y) break;
+    // intervals are sorted by sqrt_hi, descending: p reaches the first n_reach of them
+    uint32_t lo = 0, hi = n_iv;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (s_iv[mid].sqrt_hi >= p) lo = mid + 1; else hi = mid;
+    }
+    const uint32_t n_reach = lo;
+    for (uint32_t s = 0; s < n_reach; ++s) {
+      // one 16-byte load per pair: (vbase_d, vbase_lo, span32)
+      const uint4 h = *reinterpret_cast<const uint4*>(&s_iv[s]);
+      const double vd = __hiloint2double((int)h.y, (int)h.x);
       const unsigned long long q = __double2ull_rz(vd * inv);
       uint32_t d;  // first multiple of p, offset from vbase
       if (narrow) {  // 32-bit arithmetic: r = vbase - q p as int32 in (-p, 2p)
-        uint32_t r = lo_sq.x - (uint32_t)q * p;
+        uint32_t r = h.z - (uint32_t)q * p;
         r += (int32_t)r < 0 ? p : 0u;
         r -= r >= p ? p : 0u;
         d = r ? p - r : 0u;
@@ -1073,8 +1076,8 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
         rr -= rr >= (int64_t)p ? (int64_t)p : 0;
         d = rr ? p - (uint32_t)rr : 0u;
       }
-      const uint2 sp_lt = *reinterpret_cast<const uint2*>(&s_iv[s].span32);  // (span32, lt32)
-      if (d >= sp_lt.x) continue;                      // none in the interval
+      if (d >= h.w) continue;                      // none in the interval
+      const uint2 sp_lt = make_uint2(h.w, s_iv[s].lt32);
       const IntervalScatter& I = s_iv[s];
       if (sp_lt.y) {
         // wheel walk over the multiples p*m with gcd(m, 30) = 1 (vbase is a multiple of 30)

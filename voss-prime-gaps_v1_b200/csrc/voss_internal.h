@@ -75,14 +75,14 @@ struct IntervalDev {
 };
 
 // One interval as seen by the large-prime pre-pass (sorted by sqrt_hi, descending).
-struct IntervalScatter {
+struct __align__(16) IntervalScatter {
   // vbase = 30 * k0, the integer at bit 0 of the interval's first word.
   // Read for every (prime, interval) pair: 16 B
   double vbase_d;     // vbase rounded to double (for the quotient estimate of vbase mod p)
   uint32_t vbase_lo;  // low 32 bits of vbase (the remainder needs only those, see scatter_large_kernel)
-  uint32_t sqrt_hi;   // isqrt(hi - 1), capped to 2^32 - 1
-  // read when a multiple of p may lie inside
   uint32_t span32;    // min(span, 2^32 - 1)
+  // read once per prime (how many intervals it reaches) or when a multiple of p may lie inside
+  uint32_t sqrt_hi;   // isqrt(hi - 1), capped to 2^32 - 1
   uint32_t lt32;      // bytes of the interval's bitmap (span / 30) when below 2^31, else 0
   uint64_t span;      // integers covered by the interval's words (120 per word)
   uint64_t gword;     // first word in the large-prime bitmap

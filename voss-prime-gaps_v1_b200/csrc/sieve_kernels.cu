@@ -104,6 +104,32 @@ __device__ __forceinline__ uint32_t count_lt(const uint32_t* pr, uint32_t n, uin
   return count_le(pr, n, v - 1);
 }
 
+// number of table primes <= v, found by the 32 lanes of a warp together: each round probes 32
+// evenly spaced entries of the remaining range and keeps the slice between the last probe <= v
+// and the first > v, so a table of n primes takes about log32(n) rounds of loads instead of
+// log2(n) dependent ones.  Every lane returns the count.
+__device__ __forceinline__ uint32_t count_le_warp(const uint32_t* pr, uint32_t n, uint64_t v, uint32_t lane) {
+  if (v >= 0xFFFFFFFFull) return n;
+  const uint32_t x = (uint32_t)v;
+  uint32_t lo = 0, hi = n;  // the count lies in [lo, hi]
+  while (hi - lo > 32u) {
+    const uint32_t step = (hi - lo + 31u) >> 5;
+    const uint32_t pos = lo + lane * step;
+    const bool le = pos < hi && pr[pos] <= x;
+    const uint32_t k = (uint32_t)__popc(__ballot_sync(0xFFFFFFFFu, le));  // probes 0..k-1 are <= x
+    const uint32_t nlo = k ? lo + (k - 1u) * step + 1u : lo;
+    const uint32_t bound = lo + k * step;  // the first probe > x, when it exists
+    if (bound < hi) hi = bound;
+    lo = nlo;
+  }
+  const bool le = lo + lane < hi && pr[lo + lane] <= x;
+  return lo + (uint32_t)__popc(__ballot_sync(0xFFFFFFFFu, le));
+}
+
+__device__ __forceinline__ uint32_t count_lt_warp(const uint32_t* pr, uint32_t n, uint64_t v, uint32_t lane) {
+  return v == 0 ? 0u : count_le_warp(pr, n, v - 1, lane);
+}
+
 __device__ __forceinline__ uint32_t find_interval(const SieveArgs& a, uint32_t t) {
   if (a.tile_iv) return a.tile_iv[t];  // the launch's tile -> interval table
   uint32_t lo = 0, hi = a.n_intervals;  // largest i with tile_begin <= t
@@ -279,7 +305,7 @@ struct TileHdr {
   uint32_t pre_base[kPreGroups];
   uint32_t interval, tile, next_tile, cur_iv, since_flush, flush;
   uint32_t r0, r1;       // base primes lying in the tile (restore)
-  uint32_t c_lt, c_np, c_ia, c_ib, c_iw;  // category bounds of the CTA's last (tile length, np)
+  uint32_t c_lt, c_ia, c_ib, c_iw;  // category bounds over the whole table for tile length c_lt
   uint32_t coop_ctr, b_ctr, c_ctr;  // work counters of the three prime categories
   unsigned long long gword;         // the tile's first word in the large-prime bitmap
   uint32_t first;
@@ -447,7 +473,6 @@ sieve_tiles_kernel(SieveArgs a) {
     H.since_flush = 0;
     H.count_total = 0;
     H.c_lt = kNone;
-    H.c_np = kNone;
   }
   __syncthreads();
 
@@ -488,74 +513,90 @@ sieve_tiles_kernel(SieveArgs a) {
     VOSS_PHASE(0)
 
     // ---- tile header ------------------------------------------------------------------
-    if (tid == 0) {
+    // Warp 0: the lanes compute the same scalars and share the table searches (count_le_warp);
+    // lane 0 writes the header.
+    if (tid < 32) {
+      const uint32_t ln = (uint32_t)lane;
       const IntervalDev iv = a.iv[H.interval];
       const uint32_t tl = H.tile - iv.tile_begin;
       const uint64_t wofs = (uint64_t)tl * a.tile_words;
       const uint64_t nw64 = iv.n_words - wofs;
       const uint32_t nw = nw64 < a.tile_words ? (uint32_t)nw64 : a.tile_words;
       const uint64_t ktile = iv.k0 + 4ull * wofs;
-      H.cur_iv = H.interval;
-      H.ktile = ktile;
-      H.vbase = 30ull * ktile;
-      H.vlo = iv.lo;
-      H.vhi = iv.hi;
-      H.seg_k = iv.seg_k;
-      H.nw = nw;
-      H.lt = 4u * nw;
-      uint64_t vend = H.vbase + 30ull * H.lt;
+      const uint64_t vbase = 30ull * ktile;
+      const uint32_t lt = 4u * nw;
+      uint64_t vend = vbase + 30ull * lt;
       if (vend > iv.hi) vend = iv.hi;
       // table searches, skipped where the answer is known: a tile past the table's last prime
-      // needs every prime and holds none of them, and the category bounds depend only on the
-      // tile length and np, so they are kept from the CTA's previous tile when those repeat
+      // needs every prime and holds none of them; the category bounds over the whole table
+      // depend only on the tile length (count_lt over np primes = min(that, np))
       const uint64_t sq = isqrt_u64(vend - 1);
-      uint32_t np = sq >= a.p_max ? a.n_primes : count_le(a.primes, a.n_primes, sq);
+      uint32_t np = sq >= a.p_max ? a.n_primes : count_le_warp(a.primes, a.n_primes, sq, ln);
       if (a.gbm && np > a.scatter_first) np = a.scatter_first;  // the rest came from the pre-pass
-      H.np = np;
-      H.gword = iv.gword + wofs;
-      if (H.lt != H.c_lt || np != H.c_np) {
-        const uint32_t ia = count_lt(a.primes, np, (uint64_t)(H.lt / a.coop_div));
-        const uint32_t ib = count_lt(a.primes, np, (uint64_t)H.lt * a.mult_factor);
-        const uint32_t iw = count_lt(a.primes, np, ((uint64_t)H.lt * a.walk_sixteenths) >> 4);
-        H.c_ia = ia;
-        H.c_ib = ib < ia ? ia : ib;
-        H.c_iw = iw < H.c_ia ? H.c_ia : (iw > H.c_ib ? H.c_ib : iw);
-        H.c_lt = H.lt;
-        H.c_np = np;
+      if (lt != H.c_lt) {
+        const uint32_t ia = count_lt_warp(a.primes, a.n_primes, (uint64_t)(lt / a.coop_div), ln);
+        const uint32_t ib = count_lt_warp(a.primes, a.n_primes, (uint64_t)lt * a.mult_factor, ln);
+        const uint32_t iw = count_lt_warp(a.primes, a.n_primes, ((uint64_t)lt * a.walk_sixteenths) >> 4, ln);
+        __syncwarp();
+        if (ln == 0) {
+          H.c_ia = ia;
+          H.c_ib = ib;
+          H.c_iw = iw;
+          H.c_lt = lt;
+        }
+        __syncwarp();
       }
-      H.ia = H.c_ia;
-      H.ib = H.c_ib;
-      H.iw = H.c_iw;
-      if (H.vbase > a.p_max) {
-        H.r0 = H.r1 = a.n_primes;
-      } else {
-        H.r0 = count_lt(a.primes, a.n_primes, H.vbase);
-        H.r1 = count_lt(a.primes, a.n_primes, H.vbase + 30ull * H.lt);
+      const uint32_t ia = min(H.c_ia, np);
+      const uint32_t ib0 = min(H.c_ib, np);
+      const uint32_t ib = ib0 < ia ? ia : ib0;
+      const uint32_t iw0 = min(H.c_iw, np);
+      const uint32_t iw = iw0 < ia ? ia : (iw0 > ib ? ib : iw0);
+      uint32_t r0 = a.n_primes, r1 = a.n_primes;
+      if (vbase <= a.p_max) {
+        r0 = count_lt_warp(a.primes, a.n_primes, vbase, ln);
+        r1 = count_lt_warp(a.primes, a.n_primes, vbase + 30ull * lt, ln);
       }
-      uint32_t vb = kNone;
-      if (iv.seg_k) {
-        uint64_t kb = (ktile / iv.seg_k + 1) * iv.seg_k;
-        if (kb < ktile + H.lt) vb = (uint32_t)(30ull * (kb - ktile));
-      }
-      H.vb = vb;
-      // large-gap candidates: g >= cthr, one tile-uniform threshold.  Reference rule
-      // (voss_v7_live.cu:289-294): g > 100 and (g >= 500 or g / log(p) >= 10); no gap of the tile
-      // below 10 log(vbase) - 3 can reach merit 10.  With large_min_gap: g >= large_min_gap.
-      // (single-precision log: its error, a few units of 1e-6 relative at these sizes, is far
-      // inside the margin of 3; the kept gaps are then decided by the double merit below)
-      const float th = floorf(10.0f * __logf((float)(H.vbase > 7 ? H.vbase : 7))) - 3.0f;
-      uint32_t gthr = th < 0.0f ? 0u : (uint32_t)th;
-      gthr = gthr < 101u ? 101u : (gthr > 500u ? 500u : gthr);
-      H.cthr = !a.want_large ? kNone : (a.large_min_gap ? a.large_min_gap : gthr);
-      H.k28 = (uint32_t)(ktile % 28ull);
-      H.k143 = (uint32_t)(ktile % 143ull);
-      const uint64_t wt = ktile >> 2;
+      if (ln == 0) {
+        H.cur_iv = H.interval;
+        H.ktile = ktile;
+        H.vbase = vbase;
+        H.vlo = iv.lo;
+        H.vhi = iv.hi;
+        H.seg_k = iv.seg_k;
+        H.nw = nw;
+        H.lt = lt;
+        H.np = np;
+        H.gword = iv.gword + wofs;
+        H.ia = ia;
+        H.ib = ib;
+        H.iw = iw;
+        H.r0 = r0;
+        H.r1 = r1;
+        uint32_t vb = kNone;
+        if (iv.seg_k) {
+          uint64_t kb = (ktile / iv.seg_k + 1) * iv.seg_k;
+          if (kb < ktile + lt) vb = (uint32_t)(30ull * (kb - ktile));
+        }
+        H.vb = vb;
+        // large-gap candidates: g >= cthr, one tile-uniform threshold.  Reference rule
+        // (voss_v7_live.cu:289-294): g > 100 and (g >= 500 or g / log(p) >= 10); no gap of the
+        // tile below 10 log(vbase) - 3 can reach merit 10.  With large_min_gap: g >= large_min_gap.
+        // (single-precision log: its error, a few units of 1e-6 relative at these sizes, is far
+        // inside the margin of 3; the kept gaps are then decided by the double merit below)
+        const float th = floorf(10.0f * __logf((float)(vbase > 7 ? vbase : 7))) - 3.0f;
+        uint32_t gthr = th < 0.0f ? 0u : (uint32_t)th;
+        gthr = gthr < 101u ? 101u : (gthr > 500u ? 500u : gthr);
+        H.cthr = !a.want_large ? kNone : (a.large_min_gap ? a.large_min_gap : gthr);
+        H.k28 = (uint32_t)(ktile % 28ull);
+        H.k143 = (uint32_t)(ktile % 143ull);
+        const uint64_t wt = ktile >> 2;
 #pragma unroll
-      for (int g = 0; g < kPreGroups; ++g) H.pre_base[g] = (uint32_t)(wt % pre_mod(g));
-      H.coop_ctr = 0;
-      H.b_ctr = 0;
-      H.c_ctr = 0;
-      H.first = kNone;
+        for (int g = 0; g < kPreGroups; ++g) H.pre_base[g] = (uint32_t)(wt % pre_mod(g));
+        H.coop_ctr = 0;
+        H.b_ctr = 0;
+        H.c_ctr = 0;
+        H.first = kNone;
+      }
     }
     __syncthreads();
     VOSS_PHASE(1)
@@ -1059,6 +1100,7 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
       if (s_iv[mid].sqrt_hi >= p) lo = mid + 1; else hi = mid;
     }
     const uint32_t n_reach = lo;
+#pragma unroll 4
     for (uint32_t s = 0; s < n_reach; ++s) {
       // one 16-byte load per pair: (vbase_d, vbase_lo, span32)
       const uint4 h = *reinterpret_cast<const uint4*>(&s_iv[s]);

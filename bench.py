@@ -241,7 +241,7 @@ def interval_work(lo, hi, p_large: int, mr_route: int = 50) -> dict:
             if sel.size:
                 hits[c] += float(((b - sel * sel) / sel).sum())
     # (prime, interval) pairs of the large-prime pre-pass: primes p_large <= p <= isqrt(hi - 1) of
-    # every interval the library sieves (those with more such primes than mr_route times their
+    # every interval the library sieves (those with more base primes than mr_route times their
     # length go to Miller-Rabin instead, the rule of voss_sieve_intervals)
     n_large_lt = int(np.searchsorted(P, float(p_large), side="left"))
     pairs = routed = 0
@@ -250,11 +250,10 @@ def interval_work(lo, hi, p_large: int, mr_route: int = 50) -> dict:
         if b <= a7:
             continue
         np_hi = int(np.searchsorted(P, math.isqrt(b - 1), side="right"))
-        cnt = max(0, np_hi - n_large_lt)
-        if mr_route != 0xFFFFFFFF and b - a7 < (1 << 31) and cnt // mr_route > b - a7:
+        if mr_route != 0xFFFFFFFF and b - a7 < (1 << 31) and np_hi // mr_route > b - a7:
             routed += 1
             continue
-        pairs += cnt
+        pairs += max(0, np_hi - n_large_lt)
     k = 8.0 / 30.0
     return {"first_hit_offsets": int(offsets), "presieve_primes_hits": k * hits[0],
             "tile_hits": k * hits[1], "prepass_hits": k * hits[2], "p_large": int(p_large),

@@ -437,13 +437,10 @@ int stage_out(voss_ctx* c, void* dst, const void* d_src, size_t bytes, cudaStrea
 void route_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, uint32_t n, uint64_t cand_cap,
                      IntervalRoute* R) {
   NvtxRange r("route");
-  // An interval whose base primes at or above the large-prime threshold outnumber mr_route
-  // times its length costs more in per-prime reductions than Miller-Rabin of its wheel integers
-  // (about 30 Montgomery products per integer) costs; it goes to short_iv.cu.
-  const uint64_t p_large = (uint64_t)c->tune.mult_factor * 4ull * c->tune.block_threads * c->tune.chunk_words;
-  const size_t jl = (size_t)(std::lower_bound(c->primes.begin(), c->primes.end(),
-                                              (uint32_t)std::min<uint64_t>(p_large, 0xFFFFFFFFull)) -
-                             c->primes.begin());
+  // An interval whose base primes outnumber mr_route times its length costs more in per-prime
+  // reductions (one per prime in the pre-pass or in its tiles: a short interval is one partial
+  // tile, for which every prime above 8 tile lengths is a "large" prime) than Miller-Rabin of
+  // its wheel integers costs; it goes to short_iv.cu.
   const uint64_t route = c->tune.mr_route;
   for (uint32_t i = 0; i < n; ++i) {
     const uint64_t a = std::max<uint64_t>(lo[i], 7);
@@ -453,7 +450,7 @@ void route_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, 
       const size_t np = (size_t)(std::upper_bound(c->primes.begin(), c->primes.end(),
                                                   (uint32_t)std::min<uint64_t>(sq, 0xFFFFFFFFull)) -
                                  c->primes.begin());
-      const uint64_t pairs = np > jl ? np - jl : 0;
+      const uint64_t pairs = np;
       const uint64_t len = hi[i] - a;
       mr = len < (1ull << 31) && pairs / route > len && R->n_cand + len <= cand_cap;
     }

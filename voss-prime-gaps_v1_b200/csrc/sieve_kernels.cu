@@ -299,17 +299,20 @@ __device__ unsigned long long g_phase_cycles[16];
 #define VOSS_PHASE(k)
 #endif
 
-struct TileHdr {
+struct TileHdr {  // one tile's header (double-buffered: the next tile's is built during this one)
   unsigned long long ktile, vbase, vlo, vhi, seg_k;
   uint32_t nw, lt, np, ia, ib, iw, vb, cthr, k28, k143;
   uint32_t pre_base[kPreGroups];
-  uint32_t interval, tile, next_tile, cur_iv, since_flush, flush;
+  uint32_t interval, tile;
   uint32_t r0, r1;       // base primes lying in the tile (restore)
-  uint32_t c_lt, c_ia, c_ib, c_iw;  // category bounds over the whole table for tile length c_lt
   uint32_t coop_ctr, b_ctr, c_ctr;  // work counters of the three prime categories
   unsigned long long gword;         // the tile's first word in the large-prime bitmap
   uint32_t first;
-  uint32_t tile_base_rank;
+};
+
+struct CtaState {  // what a CTA carries from tile to tile
+  uint32_t cur_iv, since_flush, flush;
+  uint32_t c_lt, c_ia, c_ib, c_iw;  // category bounds over the whole table for tile length c_lt
   unsigned long long count_total;
 };
 
@@ -438,87 +441,20 @@ constexpr uint32_t kSmallSplitDiv = VOSS_SMALL_SPLIT_DIV;
 
 constexpr uint32_t kFlushEvery = 2048;  // tiles between counter flushes (u32 headroom)
 
-template <int BLOCK, bool EMIT>
-__global__ void __launch_bounds__(BLOCK, (BLOCK == 512 ? 2 : 1))
-sieve_tiles_kernel(SieveArgs a) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  uint32_t* bm = smem;
-  uint32_t* pre = smem + a.tile_words;
-  uint32_t* cnt = pre + kPreWords;
-  __shared__ TileHdr H;
-  __shared__ BlockScratch<BLOCK> S;
-  // Wheel tables in shared memory: lanes index them by their own prime's residue, which
-  // would serialize in the constant cache.
-  __shared__ uint8_t s_step[64];
-  __shared__ int8_t s_rb[32];
-  __shared__ uint32_t s_pos[32];  // bit b of a word -> integer offset 30 * (b / 8) + W30[b % 8]
-  __shared__ uint8_t s_wstart[240];
-  __shared__ uint8_t s_wstep[64];
-  __shared__ uint32_t s_rank[EMIT ? 1 : BLOCK];   // first tile rank of each thread's chunk
-  __shared__ int32_t s_before[EMIT ? 1 : BLOCK];  // last prime before each chunk (-1: none)
-  uint32_t* err = a.error;
-
-  const int tid = threadIdx.x, lane = tid & 31;
-  for (uint32_t i = tid; i < kPreWords; i += BLOCK) pre[i] = a.pretab[i];
-  if (tid < 64) s_step[tid] = c_wheel_step[tid];
-  if (tid < 32) s_rb[tid] = c_res_bit[tid];
-  if (tid < 32) s_pos[tid] = 30u * ((uint32_t)tid >> 3) + w30((uint32_t)tid & 7u);
-  if (tid < 240) s_wstart[tid] = c_walk_start[tid];
-  if (tid < 64) s_wstep[tid] = c_walk_step[tid];
-  if (!EMIT)
-    for (uint32_t i = tid; i < (uint32_t)kSmCounters; i += BLOCK) cnt[i] = 0;
-  if (tid == 0) {
-    H.next_tile = atomicAdd(a.tile_counter, 1u);
-    H.cur_iv = kNone;
-    H.since_flush = 0;
-    H.count_total = 0;
-    H.c_lt = kNone;
-  }
-  __syncthreads();
-
-  const uint32_t C = a.chunk_words;
-#ifdef VOSS_PHASE_TIMING
-  unsigned long long ph_acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  long long ph_t = clock64();
-#endif
-
-  for (;;) {
-    // ---- claim / flush ------------------------------------------------------------------
-    if (tid == 0) {
-      uint32_t t = H.next_tile;
-      uint32_t ivx = t < a.n_tiles ? find_interval(a, t) : kNone;
-      H.tile = t;
-      H.interval = ivx;
-      H.flush = (!EMIT && H.cur_iv != kNone &&
-                 (ivx != H.cur_iv || H.since_flush >= kFlushEvery)) ? 1u : 0u;
-    }
-    __syncthreads();
-    if (H.flush) {
-      unsigned long long* acc = a.acc + (size_t)H.cur_iv * kAccStride;
-      for (uint32_t i = tid; i < (uint32_t)kSmCounters; i += BLOCK) {
-        uint32_t v = cnt[i];
-        if (v) {
-          atomicAdd(acc + acc_index(i), (unsigned long long)v);
-          cnt[i] = 0;
-        }
+// The header of tile t, built by one warp: the lanes compute the same scalars and share the
+// table searches (count_le_warp); lane 0 writes the header.  t >= n_tiles marks the end.
+__device__ __forceinline__ void tile_header(TileHdr& H, CtaState& St, const SieveArgs& a, uint32_t t,
+                                            uint32_t ln) {
+  {
+    {
+      const uint32_t ivx = t < a.n_tiles ? find_interval(a, t) : kNone;
+      if (ln == 0) {
+        H.tile = t;
+        H.interval = ivx;
       }
-      if (tid == 0) {
-        atomicAdd(acc + kAccCount, H.count_total);
-        H.count_total = 0;
-        H.since_flush = 0;
-      }
-      __syncthreads();
-    }
-    if (H.tile >= a.n_tiles) break;
-    VOSS_PHASE(0)
-
-    // ---- tile header ------------------------------------------------------------------
-    // Warp 0: the lanes compute the same scalars and share the table searches (count_le_warp);
-    // lane 0 writes the header.
-    if (tid < 32) {
-      const uint32_t ln = (uint32_t)lane;
-      const IntervalDev iv = a.iv[H.interval];
-      const uint32_t tl = H.tile - iv.tile_begin;
+      if (t >= a.n_tiles) return;
+      const IntervalDev iv = a.iv[ivx];
+      const uint32_t tl = t - iv.tile_begin;
       const uint64_t wofs = (uint64_t)tl * a.tile_words;
       const uint64_t nw64 = iv.n_words - wofs;
       const uint32_t nw = nw64 < a.tile_words ? (uint32_t)nw64 : a.tile_words;
@@ -533,23 +469,23 @@ sieve_tiles_kernel(SieveArgs a) {
       const uint64_t sq = isqrt_u64(vend - 1);
       uint32_t np = sq >= a.p_max ? a.n_primes : count_le_warp(a.primes, a.n_primes, sq, ln);
       if (a.gbm && np > a.scatter_first) np = a.scatter_first;  // the rest came from the pre-pass
-      if (lt != H.c_lt) {
+      if (lt != St.c_lt) {
         const uint32_t ia = count_lt_warp(a.primes, a.n_primes, (uint64_t)(lt / a.coop_div), ln);
         const uint32_t ib = count_lt_warp(a.primes, a.n_primes, (uint64_t)lt * a.mult_factor, ln);
         const uint32_t iw = count_lt_warp(a.primes, a.n_primes, ((uint64_t)lt * a.walk_sixteenths) >> 4, ln);
         __syncwarp();
         if (ln == 0) {
-          H.c_ia = ia;
-          H.c_ib = ib;
-          H.c_iw = iw;
-          H.c_lt = lt;
+          St.c_ia = ia;
+          St.c_ib = ib;
+          St.c_iw = iw;
+          St.c_lt = lt;
         }
         __syncwarp();
       }
-      const uint32_t ia = min(H.c_ia, np);
-      const uint32_t ib0 = min(H.c_ib, np);
+      const uint32_t ia = min(St.c_ia, np);
+      const uint32_t ib0 = min(St.c_ib, np);
       const uint32_t ib = ib0 < ia ? ia : ib0;
-      const uint32_t iw0 = min(H.c_iw, np);
+      const uint32_t iw0 = min(St.c_iw, np);
       const uint32_t iw = iw0 < ia ? ia : (iw0 > ib ? ib : iw0);
       uint32_t r0 = a.n_primes, r1 = a.n_primes;
       if (vbase <= a.p_max) {
@@ -557,7 +493,6 @@ sieve_tiles_kernel(SieveArgs a) {
         r1 = count_lt_warp(a.primes, a.n_primes, vbase + 30ull * lt, ln);
       }
       if (ln == 0) {
-        H.cur_iv = H.interval;
         H.ktile = ktile;
         H.vbase = vbase;
         H.vlo = iv.lo;
@@ -598,7 +533,89 @@ sieve_tiles_kernel(SieveArgs a) {
         H.first = kNone;
       }
     }
+  }
+}
+
+template <int BLOCK, bool EMIT>
+__global__ void __launch_bounds__(BLOCK, (BLOCK == 512 ? 2 : 1))
+sieve_tiles_kernel(SieveArgs a) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* bm = smem;
+  uint32_t* pre = smem + a.tile_words;
+  uint32_t* cnt = pre + kPreWords;
+  __shared__ TileHdr HH[2];  // this tile's header and the next one's
+  __shared__ CtaState St;
+  __shared__ BlockScratch<BLOCK> S;
+  // Wheel tables in shared memory: lanes index them by their own prime's residue, which
+  // would serialize in the constant cache.
+  __shared__ uint8_t s_step[64];
+  __shared__ int8_t s_rb[32];
+  __shared__ uint32_t s_pos[32];  // bit b of a word -> integer offset 30 * (b / 8) + W30[b % 8]
+  __shared__ uint8_t s_wstart[240];
+  __shared__ uint8_t s_wstep[64];
+  __shared__ uint32_t s_rank[EMIT ? 1 : BLOCK];   // first tile rank of each thread's chunk
+  __shared__ int32_t s_before[EMIT ? 1 : BLOCK];  // last prime before each chunk (-1: none)
+  uint32_t* err = a.error;
+
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (uint32_t i = tid; i < kPreWords; i += BLOCK) pre[i] = a.pretab[i];
+  if (tid < 64) s_step[tid] = c_wheel_step[tid];
+  if (tid < 32) s_rb[tid] = c_res_bit[tid];
+  if (tid < 32) s_pos[tid] = 30u * ((uint32_t)tid >> 3) + w30((uint32_t)tid & 7u);
+  if (tid < 240) s_wstart[tid] = c_walk_start[tid];
+  if (tid < 64) s_wstep[tid] = c_walk_step[tid];
+  if (!EMIT)
+    for (uint32_t i = tid; i < (uint32_t)kSmCounters; i += BLOCK) cnt[i] = 0;
+  if (tid == 0) {
+    St.cur_iv = kNone;
+    St.since_flush = 0;
+    St.count_total = 0;
+    St.c_lt = kNone;
+  }
+  __syncthreads();
+  if (tid < 32) {  // the first tile: claim and header
+    uint32_t t0 = 0;
+    if (lane == 0) t0 = atomicAdd(a.tile_counter, 1u);
+    tile_header(HH[0], St, a, __shfl_sync(0xFFFFFFFFu, t0, 0), (uint32_t)lane);
+  }
+  __syncthreads();
+  uint32_t cur = 0;
+
+  const uint32_t C = a.chunk_words;
+#ifdef VOSS_PHASE_TIMING
+  unsigned long long ph_acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  long long ph_t = clock64();
+#endif
+
+  for (;;) {
+    TileHdr& H = HH[cur];  // built during the previous tile (or before the loop)
+    // ---- flush ------------------------------------------------------------------------
+    if (tid == 0) {
+      const uint32_t ivx = H.tile < a.n_tiles ? H.interval : kNone;
+      St.flush = (!EMIT && St.cur_iv != kNone &&
+                  (ivx != St.cur_iv || St.since_flush >= kFlushEvery)) ? 1u : 0u;
+    }
     __syncthreads();
+    if (St.flush) {
+      unsigned long long* acc = a.acc + (size_t)St.cur_iv * kAccStride;
+      for (uint32_t i = tid; i < (uint32_t)kSmCounters; i += BLOCK) {
+        uint32_t v = cnt[i];
+        if (v) {
+          atomicAdd(acc + acc_index(i), (unsigned long long)v);
+          cnt[i] = 0;
+        }
+      }
+      if (tid == 0) {
+        atomicAdd(acc + kAccCount, St.count_total);
+        St.count_total = 0;
+        St.since_flush = 0;
+      }
+      __syncthreads();
+    }
+    if (H.tile >= a.n_tiles) break;
+    if (tid == 0) St.cur_iv = H.interval;
+    VOSS_PHASE(0)
+
     VOSS_PHASE(1)
 
     const uint32_t nw = H.nw, Lt = H.lt;
@@ -631,6 +648,15 @@ sieve_tiles_kernel(SieveArgs a) {
     }
     __syncthreads();
     VOSS_PHASE(2)
+
+    // Warp 0 claims the next tile and builds its header now, while the other warps start on
+    // this tile's small primes (claimed dynamically, so they take over warp 0's share): the
+    // header's dependent loads no longer hold the whole CTA at a barrier between tiles.
+    if (tid < 32) {
+      uint32_t tn = 0;
+      if (lane == 0) tn = atomicAdd(a.tile_counter, 1u);
+      tile_header(HH[cur ^ 1u], St, a, __shfl_sync(0xFFFFFFFFu, tn, 0), (uint32_t)lane);
+    }
 
     // ---- 2. sieve ----------------------------------------------------------------------
     {
@@ -866,9 +892,9 @@ sieve_tiles_kernel(SieveArgs a) {
           if (small || g < 2u * kHistBins) {
             sm_add(cnt, (small ? mq_prev : (uint32_t)kSmHist) + (g >> 1), err);
           } else {
-            atomicAdd(a.acc + (size_t)H.cur_iv * kAccStride + kAccHistOver, 1ull);
+            atomicAdd(a.acc + (size_t)H.interval * kAccStride + kAccHistOver, 1ull);
             const uint32_t slot = atomicAdd(a.over_count, 1u);
-            if (slot < a.over_cap) a.over[slot] = OverflowGap{H.cur_iv, g};
+            if (slot < a.over_cap) a.over[slot] = OverflowGap{H.interval, g};
             else atomicOr(err, kErrOverflowList);
           }
           mlo = g > mg ? (uint32_t)prev : mlo;
@@ -880,7 +906,7 @@ sieve_tiles_kernel(SieveArgs a) {
               const uint32_t slot = atomicAdd(a.large_count, 1u);
               if (slot < a.large_cap) {
                 a.large[slot] = LargeGapDev{H.vbase + pos, (int32_t)g, (float)merit_d};
-                a.large_iv[slot] = H.cur_iv;
+                a.large_iv[slot] = H.interval;
               }
             }
           }
@@ -908,11 +934,11 @@ sieve_tiles_kernel(SieveArgs a) {
         P.bgap = 0;
         P.bgap_lo = 0;
         a.partials[H.tile] = P;
-        H.count_total += tile_cnt;
-        H.since_flush++;
+        St.count_total += tile_cnt;
+        St.since_flush++;
       }
     }
-    if (tid == 0) H.next_tile = atomicAdd(a.tile_counter, 1u);
+    cur ^= 1u;
     __syncthreads();
     VOSS_PHASE(9)
   }

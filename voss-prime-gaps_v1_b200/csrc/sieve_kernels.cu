@@ -630,6 +630,7 @@ sieve_tiles_kernel(SieveArgs a) {
       }
       const uint64_t vbase = H.vbase, vlo = H.vlo, vhi = H.vhi;
       const uint32_t* gbm = a.gbm ? a.gbm + H.gword : nullptr;
+#pragma unroll 4
       for (uint32_t w = tid; w < a.tile_words; w += BLOCK) {
         uint32_t m = 0;
         if (w < nw) {

@@ -241,24 +241,15 @@ __device__ __forceinline__ void clear_progression(uint32_t* bm, uint32_t byte, u
 // Clears every multiple p*m (gcd(m, 30) = 1) of prime p = 30a + W30[bi] in the tile whose first
 // integer is vbase (a multiple of 30) and whose length is Lt bytes, visiting only those multiples
 // (about 8*Lt/p of them) instead of eight residue progressions.  rv = vbase mod p.
-// The first multiple p*m (gcd(m, 30) = 1) of prime p = 30a + W30[bi] at or above a tile whose
-// first integer is vbase (a multiple of 30), rv = vbase mod p: its byte in the tile and the
-// wheel index of m.
-__device__ __forceinline__ void wheel_walk_start(uint32_t p, uint32_t bi, uint32_t rv, const uint8_t* s_wstart,
-                                                 uint32_t* byte, uint32_t* j) {
+__device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t p, uint32_t a, uint32_t bi, uint32_t rv,
+                                                 const uint8_t* s_wstart, const uint8_t* s_wstep,
+                                                 uint32_t Lt, uint32_t nw, uint32_t* err) {
   uint32_t off = rv ? p - rv : 0u;         // first multiple of p at or above vbase, as an offset
   const uint32_t t = off - 30u * (off / 30u);
   const uint32_t st = s_wstart[bi * 30u + t];
   off += (st & 7u) * p;                     // first multiple with m coprime to 30
-  *j = st >> 3;
-  *byte = off / 30u;
-}
-
-// Clears every multiple p*m (gcd(m, 30) = 1) of p from byte `byte` (wheel index j) to the end of
-// the tile (Lt bytes), visiting only those multiples (about 8*Lt/p of them) instead of eight
-// residue progressions; on return byte and j are the first multiple past the tile.
-__device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t a, uint32_t bi, uint32_t& byte, uint32_t& j,
-                                                 const uint8_t* s_wstep, uint32_t Lt, uint32_t nw, uint32_t* err) {
+  uint32_t j = st >> 3;
+  uint32_t byte = off / 30u;
   const uint8_t* row = s_wstep + bi * 8u;
   while (byte < Lt) {
     const uint32_t e = row[j];
@@ -317,36 +308,13 @@ struct TileHdr {  // one tile's header (double-buffered: the next tile's is buil
   uint32_t coop_ctr, b_ctr, c_ctr;  // work counters of the three prime categories
   unsigned long long gword;         // the tile's first word in the large-prime bitmap
   uint32_t first;
-  uint32_t full;      // a full-length tile: its walk primes store their state for the next one
-  uint32_t carry_np;  // walk primes with index < carry_np continue from the stored state
-  uint32_t wbase;     // index of the first walk prime of a full tile (walk_state slot 0)
 };
 
 struct CtaState {  // what a CTA carries from tile to tile
   uint32_t cur_iv, since_flush, flush;
   uint32_t c_lt, c_ia, c_ib, c_iw;  // category bounds over the whole table for tile length c_lt
-  uint32_t run_next, run_end;       // the CTA's current run of consecutive tiles
-  uint32_t last_tile, last_iv, last_np, last_full;  // the tile whose header was built last
   unsigned long long count_total;
 };
-
-// The next tile of the CTA, taken by warp 0: the next one of its current run, else the first of
-// a new run of run_tiles claimed from the work counter.  Every lane returns it.
-__device__ __forceinline__ uint32_t claim_tile(CtaState& St, const SieveArgs& a, uint32_t ln) {
-  uint32_t t = St.run_next;
-  const bool fresh = t >= St.run_end;
-  uint32_t b = 0;
-  if (fresh && ln == 0) b = atomicAdd(a.tile_counter, a.run_tiles);
-  b = __shfl_sync(0xFFFFFFFFu, b, 0);
-  if (fresh) t = b;
-  __syncwarp();
-  if (ln == 0) {
-    if (fresh) St.run_end = b + a.run_tiles;
-    St.run_next = t + 1u;
-  }
-  __syncwarp();
-  return t;
-}
 
 template <int BLOCK>
 struct BlockScratch {
@@ -519,20 +487,6 @@ __device__ __forceinline__ void tile_header(TileHdr& H, CtaState& St, const Siev
       const uint32_t ib = ib0 < ia ? ia : ib0;
       const uint32_t iw0 = min(St.c_iw, np);
       const uint32_t iw = iw0 < ia ? ia : (iw0 > ib ? ib : iw0);
-      // walk-state carry: this tile follows, in the same interval, the full tile this CTA
-      // built last (so processed last), and is full itself (same categories, same slots)
-      const bool full = lt == 4u * a.tile_words;
-      const bool carry = a.walk_state != nullptr && full && St.last_full != 0u && St.last_tile + 1u == t &&
-                         St.last_iv == ivx;
-      const uint32_t carry_np = carry ? St.last_np : 0u;
-      __syncwarp();
-      if (ln == 0) {
-        St.last_tile = t;
-        St.last_iv = ivx;
-        St.last_np = np;
-        St.last_full = full ? 1u : 0u;
-      }
-      __syncwarp();
       uint32_t r0 = a.n_primes, r1 = a.n_primes;
       if (vbase <= a.p_max) {
         r0 = count_lt_warp(a.primes, a.n_primes, vbase, ln);
@@ -553,9 +507,6 @@ __device__ __forceinline__ void tile_header(TileHdr& H, CtaState& St, const Siev
         H.iw = iw;
         H.r0 = r0;
         H.r1 = r1;
-        H.full = full && a.walk_state != nullptr ? 1u : 0u;
-        H.carry_np = carry_np;
-        H.wbase = St.c_iw;
         uint32_t vb = kNone;
         if (iv.seg_k) {
           uint64_t kb = (ktile / iv.seg_k + 1) * iv.seg_k;
@@ -620,16 +571,12 @@ sieve_tiles_kernel(SieveArgs a) {
     St.since_flush = 0;
     St.count_total = 0;
     St.c_lt = kNone;
-    St.run_next = 0;
-    St.run_end = 0;
-    St.last_tile = kNone;
-    St.last_iv = kNone;
-    St.last_np = 0;
-    St.last_full = 0;
   }
   __syncthreads();
   if (tid < 32) {  // the first tile: claim and header
-    tile_header(HH[0], St, a, claim_tile(St, a, (uint32_t)lane), (uint32_t)lane);
+    uint32_t t0 = 0;
+    if (lane == 0) t0 = atomicAdd(a.tile_counter, 1u);
+    tile_header(HH[0], St, a, __shfl_sync(0xFFFFFFFFu, t0, 0), (uint32_t)lane);
   }
   __syncthreads();
   uint32_t cur = 0;
@@ -707,7 +654,9 @@ sieve_tiles_kernel(SieveArgs a) {
     // this tile's small primes (claimed dynamically, so they take over warp 0's share): the
     // header's dependent loads no longer hold the whole CTA at a barrier between tiles.
     if (tid < 32) {
-      tile_header(HH[cur ^ 1u], St, a, claim_tile(St, a, (uint32_t)lane), (uint32_t)lane);
+      uint32_t tn = 0;
+      if (lane == 0) tn = atomicAdd(a.tile_counter, 1u);
+      tile_header(HH[cur ^ 1u], St, a, __shfl_sync(0xFFFFFFFFu, tn, 0), (uint32_t)lane);
     }
 
     // ---- 2. sieve ----------------------------------------------------------------------
@@ -756,30 +705,10 @@ sieve_tiles_kernel(SieveArgs a) {
           if (base >= ib - ia) break;
           const uint32_t i = ia + base + (uint32_t)lane;
           if (i >= iw && i < ib) {
-            // few hits per tile: walk the prime's coprime multiples, from where it stopped in the
-            // CTA's previous tile when that one was the tile before this one
+            // few hits per tile: walk the prime's coprime multiples
             const uint32_t p = a.primes[i];
             const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
-            uint32_t* ws = nullptr;
-            if (H.full) {
-              ws = a.walk_state + (size_t)blockIdx.x * a.walk_stride + (i - H.wbase);
-#ifdef VOSS_BOUNDS_CHECK
-              if (i < H.wbase || i - H.wbase >= a.walk_stride) {
-                atomicOr(err, kErrBounds);
-                ws = nullptr;
-              }
-#endif
-            }
-            uint32_t byte, j;
-            if (ws && i < H.carry_np) {
-              const uint32_t v = *ws;
-              byte = v >> 3;
-              j = v & 7u;
-            } else {
-              wheel_walk_start(p, bi, mod_barrett(H.vbase, p, a.magic[i]), s_wstart, &byte, &j);
-            }
-            clear_wheel_walk(bm, pa, bi, byte, j, s_wstep, Lt, nw, err);
-            if (ws) *ws = ((byte - Lt) << 3) | j;
+            clear_wheel_walk(bm, p, pa, bi, mod_barrett(H.vbase, p, a.magic[i]), s_wstart, s_wstep, Lt, nw, err);
           } else if (i < ib) {
             const uint32_t p = a.primes[i];
             const uint32_t r = mod_barrett(ktile, p, a.magic[i]);

@@ -233,27 +233,6 @@ int launch_plan_ws(voss_ctx* c, Workspace& W, const LaunchEvents& E, const RunPl
   const size_t smem = sieve_smem_bytes(tw);
   const int slots = c->sm_count * c->ctas_per_sm;
   const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(P.n_tiles, (uint32_t)slots));
-  // Runs of consecutive tiles per claim, with the walk primes' positions carried from tile to
-  // tile inside a run (one u32 per walk prime and CTA), when there are enough tiles for runs to
-  // leave the load balanced (at least 32 runs per CTA); the context's own launches only (the
-  // server's slots never allocate while serving).
-  a.run_tiles = 1;
-  if (!emit && &W == &c->ws && c->tune.medium_mode == 0) {
-    const uint32_t runs = (uint32_t)std::min<uint64_t>(8, P.n_tiles / (32ull * (uint64_t)grid));
-    const uint64_t lt = 4ull * tw;
-    const uint64_t p_lo = (lt * c->tune.walk_sixteenths) >> 4, p_hi = lt * c->tune.mult_factor;
-    auto below = [&](uint64_t v) {
-      return (size_t)(std::lower_bound(c->primes.begin(), c->primes.end(),
-                                       (uint32_t)std::min<uint64_t>(v, 0xFFFFFFFFull)) - c->primes.begin());
-    };
-    const size_t stride = p_hi > p_lo ? below(p_hi) - below(p_lo) : 0;
-    if (runs >= 2 && stride) {
-      if ((rc = W.walk_state.ensure(sizeof(uint32_t) * stride * (size_t)grid))) return rc;
-      a.run_tiles = runs;
-      a.walk_stride = (uint32_t)stride;
-      a.walk_state = W.walk_state.as<uint32_t>();
-    }
-  }
   // Large-prime pre-pass: primes p >= mult_factor * tile bytes are applied once per launch
   // (prime-major) instead of once per tile, when the launch's bitmap fits the budget.
   const uint64_t p_large = (uint64_t)c->tune.mult_factor * 4ull * tw;

@@ -66,7 +66,6 @@ struct Workspace {
   DevBuf iv, partials, acc, out, large, large_iv, over, counters, istats, offsets, emit, mr_work, mr_in, mr_out;
   DevBuf gbm, scat;  // large-prime pre-pass: bitmap of the launch and its interval descriptors
   DevBuf tile_iv;    // interval of each tile, for launches of more than one interval
-  DevBuf walk_state; // walk primes' positions carried between consecutive tiles of a CTA's run
   DevBuf pg_pa, pg_gap, pg_ok;  // gap proofs: inputs and verdicts (endpoints use mr_in / mr_out / mr_work)
   DevBuf sha_data, sha_off, sha_out;  // certificate hashing: messages, offsets, digests
   DevBuf ls_keys, ls_idx, ls_temp, ls_sorted;  // large-gap list sorted by position (large_sort.cu)

@@ -155,13 +155,6 @@ struct SieveArgs {
   uint32_t* over_count;
   uint32_t over_cap;
   uint32_t* error;
-  // walk-state carry: a CTA claims runs of run_tiles consecutive tiles, and between two
-  // consecutive full tiles of one interval a walk prime continues from where it stopped:
-  // walk_state holds, per CTA (stride walk_stride) and walk prime, (byte offset in the next
-  // tile << 3 | wheel index).  walk_state nullptr: every tile sets its walk primes up.
-  uint32_t run_tiles;
-  uint32_t walk_stride;
-  uint32_t* walk_state;
   // emit mode (voss_primes_range): primes written at out[tile_offset[t] + rank]
   const unsigned long long* tile_offset;
   unsigned long long* out;

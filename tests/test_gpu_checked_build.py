@@ -1,7 +1,7 @@
 """The bounds-checked build (libvoss_checked.so: every shared-memory index of the sieve kernel is
 checked, and a bad one is recorded in the error word instead of being accessed) runs the
-sieve's main workloads in a separate process (a range long enough for the walk-state carry
-between consecutive tiles among them): no call may report a bounds error, and every
+sieve's main workloads in a separate process (among them a range of 33,000 tiles, so that
+every CTA runs hundreds of tiles with its double-buffered tile headers): no call may report a bounds error, and every
 result must equal the product library's."""
 import json
 import os
@@ -25,7 +25,7 @@ with voss.Context(10**18 + 2 * 10**9) as ctx:
     for k in ("gap_hist", "mod4", "modq", "modq_gap"):
         h.update(np.ascontiguousarray(getattr(r, k)).tobytes())
     h.update(np.sort(r.large["position"]).tobytes())
-    # enough tiles for runs of consecutive tiles, whose walk primes carry their positions
+    # a long range: hundreds of tiles per CTA
     r2 = ctx.sieve_range(10**11, 3 * 10**11)
     for k in ("gap_hist", "mod4", "modq", "modq_gap"):
         h.update(np.ascontiguousarray(getattr(r2, k)).tobytes())

@@ -30,6 +30,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 
 #include "voss.h"
 #include "voss_internal.h"
@@ -423,7 +424,10 @@ __device__ __forceinline__ void block_reduce_tile(uint32_t cnt, unsigned long lo
 // (k mod 28) block is class c mod 28, of the (k mod 143) block class c mod 143.
 __device__ __forceinline__ uint32_t acc_index(uint32_t i) {
   if (i < (uint32_t)kSmModq) return (uint32_t)kAccHist + i;
-  if (i < (uint32_t)kSmCls28) return (uint32_t)kAccModq + (i - (uint32_t)kSmModq);
+  if (i < (uint32_t)kSmCls28) {
+    const uint32_t j = i - (uint32_t)kSmModq;  // 8 * bin + residue
+    return (uint32_t)kAccModq + (j & 7u) * (uint32_t)kModqBins + (j >> 3);
+  }
   if (i < (uint32_t)kSmCls143) {
     const uint32_t c = (i - (uint32_t)kSmCls28) >> 3;
     return (uint32_t)kAccCls28 + 8u * (c >= 28u ? c - 28u : c) + (i & 7u);
@@ -865,14 +869,16 @@ sieve_tiles_kernel(SieveArgs a) {
       uint32_t c28 = (uint32_t)kSmCls28 + 8u * ((H.k28 + 4u * w) % 28u);
       uint32_t c143 = (uint32_t)kSmCls143 + 8u * ((H.k143 + 4u * w) % 143u);
       uint32_t mg = 0, mlo = 0;
-      uint32_t mq_prev = 0;  // modq row of the previous prime
+      uint32_t o_prev = 0;  // wheel residue of the previous prime (modq counters: 8 * (g / 2) + o)
       if (prev >= 0) {
         const uint32_t kp = (uint32_t)prev / 30u;
-        mq_prev = (uint32_t)kSmModq + kModqBins * (uint32_t)s_rb[(uint32_t)prev - 30u * kp];
+        o_prev = (uint32_t)s_rb[(uint32_t)prev - 30u * kp];
       }
       uint32_t wpos = 120u * w;
-      for (uint32_t it = 0; it < n_mine; ++it) {
-        while (x == 0u) {  // the tile holds rb >= ra + it + 1 primes: w stays inside it
+      uint32_t it0 = 0;
+      if (prev < 0 && n_mine) {
+        // the tile's first prime: no predecessor in the tile (exactly one thread)
+        while (x == 0u) {
           x = bm[++w];
           wpos += 120u;
           c28 += 32u;
@@ -885,23 +891,45 @@ sieve_tiles_kernel(SieveArgs a) {
         const uint32_t pos = wpos + s_pos[b];
         sm_add(cnt, c28 + b, err);
         sm_add(cnt, c143 + b, err);
-        const uint32_t mq = (uint32_t)kSmModq + kModqBins * (b & 7u);
-        if (prev >= 0) {
-          const uint32_t g = pos - (uint32_t)prev;
-          const bool crossing = ((uint32_t)prev < vb) && (pos >= vb);
+        H.first = pos;
+        prev = (int32_t)pos;
+        o_prev = b & 7u;
+        it0 = 1;
+      }
+      uint32_t pv = (uint32_t)prev;
+      // Instantiated twice: in a tile without a segment boundary (vb = kNone, nearly all of
+      // them) the crossing test drops out of the loop.
+      auto walk = [&](auto cross_tag) {
+        constexpr bool kCross = decltype(cross_tag)::value;
+        for (uint32_t it = it0; it < n_mine; ++it) {
+          while (x == 0u) {  // the tile holds rb >= ra + it + 1 primes: w stays inside it
+            x = bm[++w];
+            wpos += 120u;
+            c28 += 32u;
+            if (c28 >= (uint32_t)kSmCls28 + 224u) c28 -= 224u;
+            c143 += 32u;
+            if (c143 >= (uint32_t)kSmCls143 + 1144u) c143 -= 1144u;
+          }
+          const uint32_t b = (uint32_t)__ffs(x) - 1u;
+          x &= x - 1u;
+          const uint32_t pos = wpos + s_pos[b];
+          sm_add(cnt, c28 + b, err);
+          sm_add(cnt, c143 + b, err);
+          const uint32_t g = pos - pv;
+          const bool crossing = kCross && (pv < vb) && (pos >= vb);
           const bool small = g < 100u && !crossing;
           if (small || g < 2u * kHistBins) {
-            sm_add(cnt, (small ? mq_prev : (uint32_t)kSmHist) + (g >> 1), err);
+            sm_add(cnt, small ? (uint32_t)kSmModq + 4u * g + o_prev : (uint32_t)kSmHist + (g >> 1), err);
           } else {
             atomicAdd(a.acc + (size_t)H.interval * kAccStride + kAccHistOver, 1ull);
             const uint32_t slot = atomicAdd(a.over_count, 1u);
             if (slot < a.over_cap) a.over[slot] = OverflowGap{H.interval, g};
             else atomicOr(err, kErrOverflowList);
           }
-          mlo = g > mg ? (uint32_t)prev : mlo;
+          mlo = g > mg ? pv : mlo;
           mg = g > mg ? g : mg;
           if (g >= cthr && !crossing) {
-            const uint64_t v0 = H.vbase + (uint32_t)prev;
+            const uint64_t v0 = H.vbase + pv;
             const double merit_d = (double)g / log((double)v0);
             if (a.large_min_gap || g >= 500u || merit_d >= 10.0) {
               const uint32_t slot = atomicAdd(a.large_count, 1u);
@@ -911,12 +939,12 @@ sieve_tiles_kernel(SieveArgs a) {
               }
             }
           }
-        } else {
-          H.first = pos;  // exactly one thread meets a prime with no predecessor in the tile
+          pv = pos;
+          o_prev = b & 7u;
         }
-        prev = (int32_t)pos;
-        mq_prev = mq;
-      }
+      };
+      if (vb == kNone) walk(std::false_type{});
+      else walk(std::true_type{});
       const unsigned long long key =
           mg ? (((unsigned long long)mg << 32) | (unsigned long long)(0xFFFFFFFFu - mlo)) : 0ull;
       uint32_t tile_cnt2;
@@ -1116,7 +1144,7 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t j = j0 + blockIdx.x * blockDim.x + threadIdx.x; j < j1; j += stride) {
     const uint32_t p = primes[j];  // >= 8 tile spans >= 2^11 (mod_by_estimate's range)
-    const double inv = 1.0 / (double)p;
+    const double inv = __drcp_rn((double)p);
     const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
     const uint8_t* row = s_wstep + bi * 8u;
     const bool narrow = p < (1u << 30);
@@ -1132,14 +1160,17 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
       // one 16-byte load per pair: (vbase_d, vbase_lo, span32)
       const uint4 h = *reinterpret_cast<const uint4*>(&s_iv[s]);
       const double vd = __hiloint2double((int)h.y, (int)h.x);
-      const unsigned long long q = __double2ull_rz(vd * inv);
+      // q = vbase / p rounded to an integer: adding 2^52 in the same rounding leaves the
+      // integer in the low mantissa bits (q < 2^52), so no conversion instruction is needed
+      const double qd = __fma_rn(vd, inv, 4503599627370496.0);
       uint32_t d;  // first multiple of p, offset from vbase
       if (narrow) {  // 32-bit arithmetic: r = vbase - q p as int32 in (-p, 2p)
-        uint32_t r = h.z - (uint32_t)q * p;
+        uint32_t r = h.z - (uint32_t)__double2loint(qd) * p;
         r += (int32_t)r < 0 ? p : 0u;
         r -= r >= p ? p : 0u;
         d = r ? p - r : 0u;
       } else {
+        const unsigned long long q = (unsigned long long)(__double_as_longlong(qd) - 0x4330000000000000ll);
         int64_t rr = (int64_t)(s_iv[s].vbase - q * (uint64_t)p);
         rr += rr < 0 ? (int64_t)p : 0;
         rr -= rr >= (int64_t)p ? (int64_t)p : 0;

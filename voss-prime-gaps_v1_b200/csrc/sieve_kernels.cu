@@ -47,8 +47,10 @@ __constant__ int8_t c_res_bit[32];
 // m mod 30 = t * p^-1 (mod 30); stored: (steps to the next m coprime to 30) | (its wheel index << 3).
 __constant__ uint8_t c_walk_start[240];
 // [bi*8 + j]: from m = 30c + W30[j] to the next coprime m, the byte index of p*m grows by
-// a*gap_j + corr (gap_j = W30[j+1] - W30[j], W30[8] = 31); stored: bit of p*m | corr << 3 | gap_j/2 << 6.
-__constant__ uint8_t c_walk_step[64];
+// a*gap_j + corr (gap_j = W30[j+1] - W30[j], W30[8] = 31); stored: .x = ~(1 << bit of p*m)
+// (rotated left by 8 * (byte & 3) it is the clear mask of that byte's lane in its word),
+// .y = gap_j | corr << 16.
+__constant__ uint2 c_walk_step[64];
 
 static int ensure_tables();
 
@@ -243,7 +245,7 @@ __device__ __forceinline__ void clear_progression(uint32_t* bm, uint32_t byte, u
 // integer is vbase (a multiple of 30) and whose length is Lt bytes, visiting only those multiples
 // (about 8*Lt/p of them) instead of eight residue progressions.  rv = vbase mod p.
 __device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t p, uint32_t a, uint32_t bi, uint32_t rv,
-                                                 const uint8_t* s_wstart, const uint8_t* s_wstep,
+                                                 const uint8_t* s_wstart, const uint2* s_wstep,
                                                  uint32_t Lt, uint32_t nw, uint32_t* err) {
   uint32_t off = rv ? p - rv : 0u;         // first multiple of p at or above vbase, as an offset
   const uint32_t t = off - 30u * (off / 30u);
@@ -251,11 +253,11 @@ __device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t p, uint3
   off += (st & 7u) * p;                     // first multiple with m coprime to 30
   uint32_t j = st >> 3;
   uint32_t byte = off / 30u;
-  const uint8_t* row = s_wstep + bi * 8u;
+  const uint2* row = s_wstep + bi * 8u;
   while (byte < Lt) {
-    const uint32_t e = row[j];
-    clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | (e & 7u))), nw, err);
-    byte += a * ((e >> 5) & 6u) + ((e >> 3) & 7u);
+    const uint2 e = row[j];
+    clear_bit_word(bm, byte >> 2, __funnelshift_l(e.x, e.x, (byte & 3u) << 3), nw, err);
+    byte += a * (e.y & 0xFFFFu) + (e.y >> 16);
     j = (j + 1u) & 7u;
   }
 }
@@ -556,7 +558,7 @@ sieve_tiles_kernel(SieveArgs a) {
   __shared__ int8_t s_rb[32];
   __shared__ uint32_t s_pos[32];  // bit b of a word -> integer offset 30 * (b / 8) + W30[b % 8]
   __shared__ uint8_t s_wstart[240];
-  __shared__ uint8_t s_wstep[64];
+  __shared__ uint2 s_wstep[64];
   __shared__ uint32_t s_rank[EMIT ? 1 : BLOCK];   // first tile rank of each thread's chunk
   __shared__ int32_t s_before[EMIT ? 1 : BLOCK];  // last prime before each chunk (-1: none)
   uint32_t* err = a.error;
@@ -1135,7 +1137,7 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
   __shared__ IntervalScatter s_iv[kScatterChunk];
   __shared__ int8_t s_rb[32];
   __shared__ uint8_t s_wstart[240];
-  __shared__ uint8_t s_wstep[64];
+  __shared__ uint2 s_wstep[64];
   if (threadIdx.x < 32) s_rb[threadIdx.x] = c_res_bit[threadIdx.x];
   if (threadIdx.x < 240) s_wstart[threadIdx.x] = c_walk_start[threadIdx.x];
   if (threadIdx.x < 64) s_wstep[threadIdx.x] = c_walk_step[threadIdx.x];
@@ -1146,7 +1148,7 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
     const uint32_t p = primes[j];  // >= 8 tile spans >= 2^11 (mod_by_estimate's range)
     const double inv = __drcp_rn((double)p);
     const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
-    const uint8_t* row = s_wstep + bi * 8u;
+    const uint2* row = s_wstep + bi * 8u;
     const bool narrow = p < (1u << 30);
     // intervals are sorted by sqrt_hi, descending: p reaches the first n_reach of them
     uint32_t lo = 0, hi = n_iv;
@@ -1188,9 +1190,9 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
         const uint32_t lt = sp_lt.y;
         uint32_t* g = gbm + I.gword;
         while (byte < lt) {
-          const uint32_t e = row[w];
-          atomicAnd(g + (byte >> 2), ~(1u << (((byte & 3u) << 3) | (e & 7u))));
-          byte += pa * ((e >> 5) & 6u) + ((e >> 3) & 7u);
+          const uint2 e = row[w];
+          atomicAnd(g + (byte >> 2), __funnelshift_l(e.x, e.x, (byte & 3u) << 3));
+          byte += pa * (e.y & 0xFFFFu) + (e.y >> 16);
           w = (w + 1u) & 7u;
         }
       } else {
@@ -1265,7 +1267,8 @@ static int ensure_tables() {
       const int bw = kW30h[bi] * kW30h[o];
       step[bi * 8 + o] = (uint8_t)((bw / 30) | (rb[bw % 30] << 5));
     }
-  uint8_t wstart[240], wstep[64];
+  uint8_t wstart[240];
+  uint2 wstep[64];
   for (int bi = 0; bi < 8; ++bi) {
     int pinv = 1;
     while ((kW30h[bi] * pinv) % 30 != 1) ++pinv;
@@ -1280,7 +1283,7 @@ static int ensure_tables() {
       const int d0 = (w * kW30h[j]) / 30;
       const int gap = (j < 7 ? kW30h[j + 1] : 31) - kW30h[j];
       const int corr = j < 7 ? (w * kW30h[j + 1]) / 30 - d0 : w + 0 - d0;  // j = 7: next m is 30(c+1) + 1
-      wstep[bi * 8 + j] = (uint8_t)(rb[(w * kW30h[j]) % 30] | (corr << 3) | ((gap / 2) << 6));
+      wstep[bi * 8 + j] = make_uint2(~(1u << rb[(w * kW30h[j]) % 30]), (uint32_t)gap | ((uint32_t)corr << 16));
     }
   }
   if (cudaMemcpyToSymbol(c_walk_start, wstart, sizeof(wstart)) != cudaSuccess) return -1;

@@ -48,7 +48,8 @@ __constant__ int8_t c_res_bit[32];
 __constant__ uint8_t c_walk_start[240];
 // [bi*8 + j]: from m = 30c + W30[j] to the next coprime m, the byte index of p*m grows by
 // a*gap_j + corr (gap_j = W30[j+1] - W30[j], W30[8] = 31); stored: .x = ~(1 << bit of p*m)
-// (rotated left by 8 * (byte & 3) it is the clear mask of that byte's lane in its word),
+// (rotated left by 8 * (byte & 3) it is the clear mask of that byte's lane in its word; the
+// funnel shift takes its count mod 32, so byte << 3 is that rotation),
 // .y = gap_j | corr << 16.
 __constant__ uint2 c_walk_step[64];
 
@@ -256,7 +257,7 @@ __device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t p, uint3
   const uint2* row = s_wstep + bi * 8u;
   while (byte < Lt) {
     const uint2 e = row[j];
-    clear_bit_word(bm, byte >> 2, __funnelshift_l(e.x, e.x, (byte & 3u) << 3), nw, err);
+    clear_bit_word(bm, byte >> 2, __funnelshift_l(e.x, e.x, byte << 3), nw, err);
     byte += a * (e.y & 0xFFFFu) + (e.y >> 16);
     j = (j + 1u) & 7u;
   }
@@ -1191,7 +1192,7 @@ __global__ void __launch_bounds__(512) scatter_large_kernel(const uint32_t* __re
         uint32_t* g = gbm + I.gword;
         while (byte < lt) {
           const uint2 e = row[w];
-          atomicAnd(g + (byte >> 2), __funnelshift_l(e.x, e.x, (byte & 3u) << 3));
+          atomicAnd(g + (byte >> 2), __funnelshift_l(e.x, e.x, byte << 3));
           byte += pa * (e.y & 0xFFFFu) + (e.y >> 16);
           w = (w + 1u) & 7u;
         }

@@ -52,6 +52,12 @@ __constant__ uint8_t c_walk_start[240];
 // funnel shift takes its count mod 32, so byte << 3 is that rotation),
 // .y = gap_j | corr << 16.
 __constant__ uint2 c_walk_step[64];
+// The same steps packed into registers for the tile kernel's walk (no table load per visit:
+// shared-memory wavefronts are as scarce as issue slots there): nibble j of [bi] is corr_j,
+// nibble j of [8 + bi] the bit of p*m, nibble j of kGap2Packed gap_j / 2; the walk rotates the
+// three words by 4 bits per step, so the current step is always nibble 0.
+__constant__ uint32_t c_walk_pk[16];
+constexpr uint32_t kGap2Packed = 0x13212123u;
 
 static int ensure_tables();
 
@@ -246,20 +252,26 @@ __device__ __forceinline__ void clear_progression(uint32_t* bm, uint32_t byte, u
 // integer is vbase (a multiple of 30) and whose length is Lt bytes, visiting only those multiples
 // (about 8*Lt/p of them) instead of eight residue progressions.  rv = vbase mod p.
 __device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t p, uint32_t a, uint32_t bi, uint32_t rv,
-                                                 const uint8_t* s_wstart, const uint2* s_wstep,
+                                                 const uint8_t* s_wstart, const uint32_t* s_wpk,
                                                  uint32_t Lt, uint32_t nw, uint32_t* err) {
   uint32_t off = rv ? p - rv : 0u;         // first multiple of p at or above vbase, as an offset
   const uint32_t t = off - 30u * (off / 30u);
   const uint32_t st = s_wstart[bi * 30u + t];
   off += (st & 7u) * p;                     // first multiple with m coprime to 30
-  uint32_t j = st >> 3;
+  const uint32_t sh = 4u * (st >> 3);
   uint32_t byte = off / 30u;
-  const uint2* row = s_wstep + bi * 8u;
+  const uint32_t c0 = s_wpk[bi], b0 = s_wpk[8u + bi];
+  uint32_t G = __funnelshift_r(kGap2Packed, kGap2Packed, sh);
+  uint32_t C = __funnelshift_r(c0, c0, sh), B = __funnelshift_r(b0, b0, sh);
+  const uint32_t a2 = 2u * a;
   while (byte < Lt) {
-    const uint2 e = row[j];
-    clear_bit_word(bm, byte >> 2, __funnelshift_l(e.x, e.x, byte << 3), nw, err);
-    byte += a * (e.y & 0xFFFFu) + (e.y >> 16);
-    j = (j + 1u) & 7u;
+    // ~(1 << bit) rotated by 8 * (byte & 3): the funnel shift takes its count mod 32, and
+    // bit < 8 leaves the byte-lane part of (byte << 3) + bit untouched
+    clear_bit_word(bm, byte >> 2, __funnelshift_l(0xFFFFFFFEu, 0xFFFFFFFEu, (byte << 3) + (B & 7u)), nw, err);
+    byte += a2 * (G & 3u) + (C & 7u);
+    G = __funnelshift_r(G, G, 4);
+    C = __funnelshift_r(C, C, 4);
+    B = __funnelshift_r(B, B, 4);
   }
 }
 
@@ -559,7 +571,7 @@ sieve_tiles_kernel(SieveArgs a) {
   __shared__ int8_t s_rb[32];
   __shared__ uint32_t s_pos[32];  // bit b of a word -> integer offset 30 * (b / 8) + W30[b % 8]
   __shared__ uint8_t s_wstart[240];
-  __shared__ uint2 s_wstep[64];
+  __shared__ uint32_t s_wpk[16];
   __shared__ uint32_t s_rank[EMIT ? 1 : BLOCK];   // first tile rank of each thread's chunk
   __shared__ int32_t s_before[EMIT ? 1 : BLOCK];  // last prime before each chunk (-1: none)
   uint32_t* err = a.error;
@@ -570,7 +582,7 @@ sieve_tiles_kernel(SieveArgs a) {
   if (tid < 32) s_rb[tid] = c_res_bit[tid];
   if (tid < 32) s_pos[tid] = 30u * ((uint32_t)tid >> 3) + w30((uint32_t)tid & 7u);
   if (tid < 240) s_wstart[tid] = c_walk_start[tid];
-  if (tid < 64) s_wstep[tid] = c_walk_step[tid];
+  if (tid < 16) s_wpk[tid] = c_walk_pk[tid];
   if (!EMIT)
     for (uint32_t i = tid; i < (uint32_t)kSmCounters; i += BLOCK) cnt[i] = 0;
   if (tid == 0) {
@@ -715,7 +727,7 @@ sieve_tiles_kernel(SieveArgs a) {
             // few hits per tile: walk the prime's coprime multiples
             const uint32_t p = a.primes[i];
             const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
-            clear_wheel_walk(bm, p, pa, bi, mod_barrett(H.vbase, p, a.magic[i]), s_wstart, s_wstep, Lt, nw, err);
+            clear_wheel_walk(bm, p, pa, bi, mod_barrett(H.vbase, p, a.magic[i]), s_wstart, s_wpk, Lt, nw, err);
           } else if (i < ib) {
             const uint32_t p = a.primes[i];
             const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
@@ -1270,6 +1282,7 @@ static int ensure_tables() {
     }
   uint8_t wstart[240];
   uint2 wstep[64];
+  uint32_t wpk[16] = {0};
   for (int bi = 0; bi < 8; ++bi) {
     int pinv = 1;
     while ((kW30h[bi] * pinv) % 30 != 1) ++pinv;
@@ -1285,10 +1298,13 @@ static int ensure_tables() {
       const int gap = (j < 7 ? kW30h[j + 1] : 31) - kW30h[j];
       const int corr = j < 7 ? (w * kW30h[j + 1]) / 30 - d0 : w + 0 - d0;  // j = 7: next m is 30(c+1) + 1
       wstep[bi * 8 + j] = make_uint2(~(1u << rb[(w * kW30h[j]) % 30]), (uint32_t)gap | ((uint32_t)corr << 16));
+      wpk[bi] |= (uint32_t)corr << (4 * j);
+      wpk[8 + bi] |= (uint32_t)rb[(w * kW30h[j]) % 30] << (4 * j);
     }
   }
   if (cudaMemcpyToSymbol(c_walk_start, wstart, sizeof(wstart)) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_walk_step, wstep, sizeof(wstep)) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(c_walk_pk, wpk, sizeof(wpk)) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_wheel_step, step, sizeof(step)) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_res_bit, rb, sizeof(rb)) != cudaSuccess) return -1;
   g_tables_ready.fetch_or(bit);

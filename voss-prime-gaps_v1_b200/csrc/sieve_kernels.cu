@@ -77,6 +77,18 @@ __device__ __forceinline__ uint32_t mod_barrett(uint64_t x, uint32_t p, uint64_t
   return (uint32_t)r;
 }
 
+// x mod p for x < 2^53 and 8 <= p < 2^30 from the Barrett constant m = floor((2^64-1)/p), with
+// xs = x * 2^-64 as a double (exact).  m rounded to double times xs is x/p within a relative
+// 2^-53 (x/p < 2^50), so adding 2^52 in the same rounding (fma) leaves an integer q within 0.63
+// of x/p in the low mantissa bits; x - q p then lies in (-p, 2p), which its low 32 bits hold.
+__device__ __forceinline__ uint32_t mod_by_magic_fma(uint64_t x, double xs, uint32_t p, uint64_t m) {
+  const double qd = __fma_rn(xs, __ull2double_rn(m), 4503599627370496.0);
+  uint32_t r = (uint32_t)x - (uint32_t)__double2loint(qd) * p;
+  r += (int32_t)r < 0 ? p : 0u;
+  r -= r >= p ? p : 0u;
+  return r;
+}
+
 // x mod p from a double-precision estimate of the quotient, for p >= 2^11 and x < 2^62:
 // xd = x and inv = 1/p rounded to double, so xd * inv is within (x/p) * 3 * 2^-53 < 2^-1 of x/p
 // and its truncation is floor(x/p) - 1, floor(x/p) or floor(x/p) + 1; one signed correction
@@ -682,6 +694,9 @@ sieve_tiles_kernel(SieveArgs a) {
     {
       const uint64_t ktile = H.ktile;
       const uint32_t ia = H.ia, ib = H.ib, iw = H.iw, np = H.np;
+      // tiles below 2^53 reduce the prime offsets with one fma instead of the 64-bit Barrett product
+      const bool fma_mod = H.vbase < (1ull << 53);
+      const double ks = (double)ktile * 0x1p-64, vs = (double)H.vbase * 0x1p-64;
       // small primes: a warp per prime
       const uint32_t split = Lt / kSmallSplitDiv;
       const uint32_t lane_ofs = 4u * (uint32_t)lane;
@@ -727,10 +742,13 @@ sieve_tiles_kernel(SieveArgs a) {
             // few hits per tile: walk the prime's coprime multiples
             const uint32_t p = a.primes[i];
             const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
-            clear_wheel_walk(bm, p, pa, bi, mod_barrett(H.vbase, p, a.magic[i]), s_wstart, s_wpk, Lt, nw, err);
+            const uint64_t m = a.magic[i];
+            clear_wheel_walk(bm, p, pa, bi, fma_mod ? mod_by_magic_fma(H.vbase, vs, p, m) : mod_barrett(H.vbase, p, m),
+                             s_wstart, s_wpk, Lt, nw, err);
           } else if (i < ib) {
             const uint32_t p = a.primes[i];
-            const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
+            const uint64_t m = a.magic[i];
+            const uint32_t r = fma_mod ? mod_by_magic_fma(ktile, ks, p, m) : mod_barrett(ktile, p, m);
             const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
 #pragma unroll
             for (uint32_t o = 0; o < 8; ++o) {
@@ -770,7 +788,8 @@ sieve_tiles_kernel(SieveArgs a) {
         const uint32_t i = ib + base + (uint32_t)lane;
         if (i < np) {
           const uint32_t p = a.primes[i];
-          const uint32_t r = mod_barrett(vbase, p, a.magic[i]);
+          const uint64_t m = a.magic[i];
+          const uint32_t r = fma_mod && p < (1u << 30) ? mod_by_magic_fma(vbase, vs, p, m) : mod_barrett(vbase, p, m);
           uint32_t d = r ? p - r : 0u;
           for (; d < span; d += p) {
             const uint32_t q = d / 30u;

@@ -228,7 +228,10 @@ __device__ __forceinline__ void clear_block_progression(uint32_t* bm, uint32_t b
     byte += 128u * p * k;
   }
   // at most three hits remain (byte + 3p >= Lt); the next block belongs to the next lane
-  for (; byte < Lt; byte += p) clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
+  {
+    const uint32_t nb = ~(1u << bit);  // rotated by 8 * (byte & 3): the funnel shift takes byte << 3 mod 32
+    for (; byte < Lt; byte += p) clear_bit_word(bm, byte >> 2, __funnelshift_l(nb, nb, byte << 3), nw, err);
+  }
 }
 
 // Clears bit `bit` of bytes byte, byte + p, byte + 2p, ... below Lt (p odd).  Four consecutive
@@ -257,7 +260,10 @@ __device__ __forceinline__ void clear_progression(uint32_t* bm, uint32_t byte, u
     }
     byte = (w0 << 2) | j0;  // the loop advanced by 4p bytes (p words) per trip
   }
-  for (; byte < Lt; byte += p) clear_bit_word(bm, byte >> 2, ~(1u << (((byte & 3u) << 3) | bit)), nw, err);
+  {
+    const uint32_t nb = ~(1u << bit);  // rotated by 8 * (byte & 3): the funnel shift takes byte << 3 mod 32
+    for (; byte < Lt; byte += p) clear_bit_word(bm, byte >> 2, __funnelshift_l(nb, nb, byte << 3), nw, err);
+  }
 }
 
 // Clears every multiple p*m (gcd(m, 30) = 1) of prime p = 30a + W30[bi] in the tile whose first
@@ -279,7 +285,7 @@ __device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t p, uint3
   while (byte < Lt) {
     // ~(1 << bit) rotated by 8 * (byte & 3): the funnel shift takes its count mod 32, and
     // bit < 8 leaves the byte-lane part of (byte << 3) + bit untouched
-    clear_bit_word(bm, byte >> 2, __funnelshift_l(0xFFFFFFFEu, 0xFFFFFFFEu, (byte << 3) + (B & 7u)), nw, err);
+    clear_bit_word(bm, byte >> 2, __funnelshift_l(0xFFFFFFFEu, 0xFFFFFFFEu, ((byte << 3) & 24u) | (B & ~24u)), nw, err);
     byte += a2 * (G & 3u) + (C & 7u);
     G = __funnelshift_r(G, G, 4);
     C = __funnelshift_r(C, C, 4);
@@ -579,7 +585,7 @@ sieve_tiles_kernel(SieveArgs a) {
   __shared__ BlockScratch<BLOCK> S;
   // Wheel tables in shared memory: lanes index them by their own prime's residue, which
   // would serialize in the constant cache.
-  __shared__ uint8_t s_step[64];
+  __shared__ __align__(8) uint8_t s_step[64];
   __shared__ int8_t s_rb[32];
   __shared__ uint32_t s_pos[32];  // bit b of a word -> integer offset 30 * (b / 8) + W30[b % 8]
   __shared__ uint8_t s_wstart[240];
@@ -750,9 +756,10 @@ sieve_tiles_kernel(SieveArgs a) {
             const uint64_t m = a.magic[i];
             const uint32_t r = fma_mod ? mod_by_magic_fma(ktile, ks, p, m) : mod_barrett(ktile, p, m);
             const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
+            const uint2 st8 = reinterpret_cast<const uint2*>(s_step)[bi];  // the prime's 8 entries
 #pragma unroll
             for (uint32_t o = 0; o < 8; ++o) {
-              const uint32_t e = s_step[bi * 8u + o];
+              const uint32_t e = ((o < 4u ? st8.x : st8.y) >> (8u * (o & 3u))) & 0xFFu;
               const uint32_t delta = pa * w30(o) + (e & 31u);
               clear_progression(bm, delta >= r ? delta - r : delta + p - r, p, e >> 5, Lt, nw, err);
             }

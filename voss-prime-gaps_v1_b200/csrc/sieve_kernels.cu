@@ -270,7 +270,7 @@ __device__ __forceinline__ void clear_progression(uint32_t* bm, uint32_t byte, u
 // integer is vbase (a multiple of 30) and whose length is Lt bytes, visiting only those multiples
 // (about 8*Lt/p of them) instead of eight residue progressions.  rv = vbase mod p.
 __device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t p, uint32_t a, uint32_t bi, uint32_t rv,
-                                                 const uint8_t* s_wstart, const uint32_t* s_wpk,
+                                                 const uint8_t* s_wstart, const uint2* s_wpk,
                                                  uint32_t Lt, uint32_t nw, uint32_t* err) {
   uint32_t off = rv ? p - rv : 0u;         // first multiple of p at or above vbase, as an offset
   const uint32_t t = off - 30u * (off / 30u);
@@ -278,7 +278,8 @@ __device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t p, uint3
   off += (st & 7u) * p;                     // first multiple with m coprime to 30
   const uint32_t sh = 4u * (st >> 3);
   uint32_t byte = off / 30u;
-  const uint32_t c0 = s_wpk[bi], b0 = s_wpk[8u + bi];
+  const uint2 cb = s_wpk[bi];
+  const uint32_t c0 = cb.x, b0 = cb.y;
   uint32_t G = __funnelshift_r(kGap2Packed, kGap2Packed, sh);
   uint32_t C = __funnelshift_r(c0, c0, sh), B = __funnelshift_r(b0, b0, sh);
   const uint32_t a2 = 2u * a;
@@ -589,7 +590,7 @@ sieve_tiles_kernel(SieveArgs a) {
   __shared__ int8_t s_rb[32];
   __shared__ uint32_t s_pos[32];  // bit b of a word -> integer offset 30 * (b / 8) + W30[b % 8]
   __shared__ uint8_t s_wstart[240];
-  __shared__ uint32_t s_wpk[16];
+  __shared__ uint2 s_wpk[8];
   __shared__ uint32_t s_rank[EMIT ? 1 : BLOCK];   // first tile rank of each thread's chunk
   __shared__ int32_t s_before[EMIT ? 1 : BLOCK];  // last prime before each chunk (-1: none)
   uint32_t* err = a.error;
@@ -600,7 +601,7 @@ sieve_tiles_kernel(SieveArgs a) {
   if (tid < 32) s_rb[tid] = c_res_bit[tid];
   if (tid < 32) s_pos[tid] = 30u * ((uint32_t)tid >> 3) + w30((uint32_t)tid & 7u);
   if (tid < 240) s_wstart[tid] = c_walk_start[tid];
-  if (tid < 16) s_wpk[tid] = c_walk_pk[tid];
+  if (tid < 8) s_wpk[tid] = make_uint2(c_walk_pk[tid], c_walk_pk[8 + tid]);
   if (!EMIT)
     for (uint32_t i = tid; i < (uint32_t)kSmCounters; i += BLOCK) cnt[i] = 0;
   if (tid == 0) {

@@ -943,6 +943,8 @@ sieve_tiles_kernel(SieveArgs a) {
       // them) the crossing test drops out of the loop.
       auto walk = [&](auto cross_tag) {
         constexpr bool kCross = decltype(cross_tag)::value;
+        // unrolled by 4: one trip-count test per four primes (the count is known at entry)
+#pragma unroll 4
         for (uint32_t it = it0; it < n_mine; ++it) {
           while (x == 0u) {  // the tile holds rb >= ra + it + 1 primes: w stays inside it
             x = bm[++w];

@@ -645,7 +645,7 @@ def run_serve(a) -> dict:
     clocks = ClockSampler(0)
     clocks.start()
     runs = []
-    for _ in range(2):  # the better of two runs: the host copies of the Miller-Rabin payloads vary
+    for _ in range(3):  # the best of three runs (all reported): host scheduling and the copies vary
         with Server(ctx) as srv:
             lat, wall, _, err = serve_stream(srv, burst)
             st = srv.stats()
@@ -663,7 +663,7 @@ def run_serve(a) -> dict:
                 "plain_req_s": plain_rps, "plain_requests_served": len(pl), "plain_wall_s": plain_wall,
                 "clocks": clk,
                 "note": "all requests offered at once (the payloads of the 1e4 req/s stream of this length); "
-                        "served = continuous batching over 4 slots, the better of two runs; plain = one launch "
+                        "served = continuous batching over 4 slots, the best of three runs; plain = one launch "
                         "per request in order (time-capped); both include the host copies of the requests"}
     top = rows[-1]
     out = {

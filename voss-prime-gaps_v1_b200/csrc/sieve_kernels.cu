@@ -219,6 +219,7 @@ __device__ __forceinline__ void clear_block_progression(uint32_t* bm, uint32_t b
     // b3 + 128 p k < Lt  <=>  (b3 >> 2) + 32 p k < lim
     const uint32_t lim = ((Lt + 3u - (b3 & 3u)) >> 2) - d3;
     uint32_t k = 0;
+#pragma unroll 2
     for (; w0 < lim; w0 += ws, ++k) {
       clear_bit_word(bm, w0, m0, nw, err);
       clear_bit_word(bm, w0 + d1, m1, nw, err);

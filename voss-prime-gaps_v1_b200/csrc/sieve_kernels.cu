@@ -190,6 +190,7 @@ __device__ __forceinline__ void clear_lane_progression(uint32_t* bm, uint32_t st
   uint32_t w = start >> 2;
   if (wlim > 3u * ws) {
     const uint32_t wlim4 = wlim - 3u * ws;
+#pragma unroll 2
     for (; w < wlim4; w += 4u * ws) {
       clear_bit_word(bm, w, mask, nw, err);
       clear_bit_word(bm, w + ws, mask, nw, err);
@@ -219,7 +220,7 @@ __device__ __forceinline__ void clear_block_progression(uint32_t* bm, uint32_t b
     // b3 + 128 p k < Lt  <=>  (b3 >> 2) + 32 p k < lim
     const uint32_t lim = ((Lt + 3u - (b3 & 3u)) >> 2) - d3;
     uint32_t k = 0;
-#pragma unroll 2
+#pragma unroll 4
     for (; w0 < lim; w0 += ws, ++k) {
       clear_bit_word(bm, w0, m0, nw, err);
       clear_bit_word(bm, w0 + d1, m1, nw, err);
@@ -860,10 +861,14 @@ sieve_tiles_kernel(SieveArgs a) {
       // pass 1: the primes of my chunk and its last prime
       uint32_t pc = 0;
       int32_t my_last = -1;
-      for (uint32_t w = c0; w < cend; ++w) {
-        const uint32_t x = bm[w];
-        pc += (uint32_t)__popc(x);
-        if (x) my_last = (int32_t)(120u * w + s_pos[31u - (uint32_t)__clz(x)]);
+#pragma unroll 7
+      for (uint32_t w = c0; w < cend; ++w) pc += (uint32_t)__popc(bm[w]);
+      for (uint32_t w = cend; pc && w > c0;) {  // the chunk's last prime: its last non-zero word
+        const uint32_t x = bm[--w];
+        if (x) {
+          my_last = (int32_t)(120u * w + s_pos[31u - (uint32_t)__clz(x)]);
+          break;
+        }
       }
       uint32_t tile_cnt;
       const uint32_t rank0 = block_excl_sum<BLOCK>(pc, S, &tile_cnt);

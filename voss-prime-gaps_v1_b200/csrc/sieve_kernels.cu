@@ -595,6 +595,7 @@ sieve_tiles_kernel(SieveArgs a) {
   __shared__ uint2 s_wpk[8];
   __shared__ uint32_t s_rank[EMIT ? 1 : BLOCK];   // first tile rank of each thread's chunk
   __shared__ int32_t s_before[EMIT ? 1 : BLOCK];  // last prime before each chunk (-1: none)
+  __shared__ uint16_t s_mid[EMIT ? 1 : BLOCK];    // primes in the first C / 2 words of each chunk
   uint32_t* err = a.error;
 
   const int tid = threadIdx.x, lane = tid & 31;
@@ -670,14 +671,19 @@ sieve_tiles_kernel(SieveArgs a) {
       }
       const uint64_t vbase = H.vbase, vlo = H.vlo, vhi = H.vhi;
       const uint32_t* gbm = a.gbm ? a.gbm + H.gword : nullptr;
+      // words [w_in, w_out) lie wholly inside [vlo, vhi) (v0 + 1 >= vlo and v0 + 120 <= vhi):
+      // only the others need an edge mask
+      const uint64_t lo_words = vlo <= vbase + 1 ? 0ull : (vlo - vbase + 118ull) / 120ull;
+      const uint64_t hi_words = vhi < vbase + 120 ? 0ull : (vhi - vbase) / 120ull;
+      const uint32_t w_in = (uint32_t)(lo_words < a.tile_words ? lo_words : a.tile_words);
+      const uint32_t w_out = (uint32_t)(hi_words < a.tile_words ? hi_words : a.tile_words);
 #pragma unroll 4
       for (uint32_t w = tid; w < a.tile_words; w += BLOCK) {
         uint32_t m = 0;
         if (w < nw) {
           m = pre[ix[0]] & pre[1001u + ix[1]] & pre[1324u + ix[2]] & pre[1991u + ix[3]];
           if (gbm) m &= gbm[w];
-          const uint64_t v0 = vbase + 120ull * w;
-          if (v0 + 1 < vlo || v0 + 120 > vhi) m &= edge_mask(v0, vlo, vhi);
+          if (w < w_in || w >= w_out) m &= edge_mask(vbase + 120ull * w, vlo, vhi);
         }
         bm[w] = m;
 #pragma unroll
@@ -861,8 +867,12 @@ sieve_tiles_kernel(SieveArgs a) {
       // pass 1: the primes of my chunk and its last prime
       uint32_t pc = 0;
       int32_t my_last = -1;
-#pragma unroll 7
-      for (uint32_t w = c0; w < cend; ++w) pc += (uint32_t)__popc(bm[w]);
+      const uint32_t cmid = c0 + (C >> 1) < cend ? c0 + (C >> 1) : cend;
+#pragma unroll 4
+      for (uint32_t w = c0; w < cmid; ++w) pc += (uint32_t)__popc(bm[w]);
+      const uint32_t pc_half = pc;
+#pragma unroll 4
+      for (uint32_t w = cmid; w < cend; ++w) pc += (uint32_t)__popc(bm[w]);
       for (uint32_t w = cend; pc && w > c0;) {  // the chunk's last prime: its last non-zero word
         const uint32_t x = bm[--w];
         if (x) {
@@ -875,6 +885,7 @@ sieve_tiles_kernel(SieveArgs a) {
       int32_t tile_last;
       const int32_t before = block_excl_max<BLOCK>(my_last, S, &tile_last);
       s_rank[tid] = rank0;
+      s_mid[tid] = (uint16_t)pc_half;
       s_before[tid] = before;
       __syncthreads();
       VOSS_PHASE(7)
@@ -894,19 +905,32 @@ sieve_tiles_kernel(SieveArgs a) {
           if (s_rank[mid] <= ra) lo = mid; else hi = mid;
         }
         uint32_t k = ra - s_rank[lo];
-        prev = s_before[lo];
         w = lo * C;
+        const uint32_t kh = s_mid[lo];
+        if (k >= kh) {  // the start lies in the chunk's second half
+          k -= kh;
+          w += C >> 1;
+        }
         x = bm[w];
         for (;;) {  // the word holding the start: it lies in chunk lo
           const uint32_t c = (uint32_t)__popc(x);
           if (k < c) break;
-          if (x) prev = (int32_t)(120u * w + s_pos[31u - (uint32_t)__clz(x)]);
           k -= c;
           x = bm[++w];
         }
-        for (; k; --k) {  // the primes of that word before mine
+        if (k) {  // the primes of that word before mine: the last of them is my predecessor
+          for (; k > 1u; --k) x &= x - 1u;
           prev = (int32_t)(120u * w + s_pos[(uint32_t)__ffs(x) - 1u]);
           x &= x - 1u;
+        } else {  // mine is the word's first prime: the predecessor is in an earlier word
+          prev = s_before[lo];
+          for (uint32_t ww = w; ww > lo * C;) {
+            const uint32_t y = bm[--ww];
+            if (y) {
+              prev = (int32_t)(120u * ww + s_pos[31u - (uint32_t)__clz(y)]);
+              break;
+            }
+          }
         }
       }
       // The class counters of a word's 4 bytes are indexed without wrapping (k mod 28 + j up to

@@ -212,8 +212,10 @@ __device__ __forceinline__ void clear_block_progression(uint32_t* bm, uint32_t b
                                                         uint32_t Lt, uint32_t nw, uint32_t* err) {
   if (byte + 3u * p < Lt) {
     const uint32_t b1 = byte + p, b2 = b1 + p, b3 = b2 + p;
-    const uint32_t m0 = ~(1u << (((byte & 3u) << 3) | bit)), m1 = ~(1u << (((b1 & 3u) << 3) | bit));
-    const uint32_t m2 = ~(1u << (((b2 & 3u) << 3) | bit)), m3 = ~(1u << (((b3 & 3u) << 3) | bit));
+    // ~(1 << bit) rotated to each byte's lane (the funnel shift takes its count mod 32)
+    const uint32_t nb = ~(1u << bit);
+    const uint32_t m0 = __funnelshift_l(nb, nb, byte << 3), m1 = __funnelshift_l(nb, nb, b1 << 3);
+    const uint32_t m2 = __funnelshift_l(nb, nb, b2 << 3), m3 = __funnelshift_l(nb, nb, b3 << 3);
     uint32_t w0 = byte >> 2;
     const uint32_t d1 = (b1 >> 2) - w0, d2 = (b2 >> 2) - w0, d3 = (b3 >> 2) - w0;
     const uint32_t ws = 32u * p;
@@ -245,11 +247,10 @@ __device__ __forceinline__ void clear_progression(uint32_t* bm, uint32_t byte, u
     // the four hits' byte lanes are j0, j0 + p, j0 + 2p, j0 + 3p (mod 4): one lane up each time
     // for p = 1 (mod 4), one lane down for p = 3, so each mask is the previous one rotated by a byte
     const uint32_t j0 = byte & 3u;
-    const uint32_t M0 = 1u << ((j0 << 3) | bit);
+    const uint32_t nb = ~(1u << bit);
     const uint32_t rot = (p & 2u) ? 24u : 8u;
-    const uint32_t M1 = __funnelshift_l(M0, M0, rot), M2 = __funnelshift_l(M1, M1, rot),
-                   M3 = __funnelshift_l(M2, M2, rot);
-    const uint32_t m0 = ~M0, m1 = ~M1, m2 = ~M2, m3 = ~M3;
+    const uint32_t m0 = __funnelshift_l(nb, nb, byte << 3), m1 = __funnelshift_l(m0, m0, rot),
+                   m2 = __funnelshift_l(m1, m1, rot), m3 = __funnelshift_l(m2, m2, rot);
     uint32_t w0 = byte >> 2;
     const uint32_t d1 = (j0 + p) >> 2, d2 = (j0 + 2u * p) >> 2, d3 = (j0 + 3u * p) >> 2;
     // b3 + 4pk < Lt  <=>  w0 + k < lim  (w0 + d3 = b3 >> 2)
@@ -721,7 +722,8 @@ sieve_tiles_kernel(SieveArgs a) {
         i = __shfl_sync(0xFFFFFFFFu, i, 0);
         if (i >= ia) break;
         const uint32_t p = a.primes[i];
-        const uint32_t r = mod_barrett(ktile, p, a.magic[i]);
+        const uint64_t m = a.magic[i];
+        const uint32_t r = fma_mod ? mod_by_magic_fma(ktile, ks, p, m) : mod_barrett(ktile, p, m);
         const uint32_t pa = p / 30u, bi = (uint32_t)s_rb[p - 30u * pa];
         if (p >= split) {
           // 4 lanes per residue progression (lane = 4 o + q: bytes s_o + q p + 4p k)

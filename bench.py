@@ -859,9 +859,10 @@ def main():
                 sh = sp["share"]
                 ext = sh["extract_scan"] + sh["extract_walk"] + sh["extract_reduce"]
                 sie = sh["fill"] + sh["small_primes"] + sh["medium_primes"] + sh["large_primes"] + sh["restore"]
-                # extraction: one 32-bit read of every bitmap word (N/30 B) + three 32-bit shared-memory
-                # RMWs per prime (gap bin and two residue-class counters, 8 B each)
-                ext_bytes = (hi - lo) / 30.0 + 24.0 * r.prime_count
+                # extraction: two 32-bit reads of every bitmap word (N/30 B each: the residue-class
+                # count by word and the in-order walk) + one 32-bit shared-memory RMW per prime (its
+                # gap bin, 8 B) + 64 RMWs per 1001 words (the class counters)
+                ext_bytes = 2.0 * (hi - lo) / 30.0 + 8.0 * r.prime_count + 8.0 * 64.0 * (hi - lo) / (120.0 * 1001.0)
                 ext_ms, sie_ms = ext * kernel_ms, sie * kernel_ms
                 out["roofline_split"] = {
                     "source": "phase shares of the tile kernel from the phase-timing build (libvoss_timing.so, "
@@ -874,7 +875,7 @@ def main():
                     "extract": {"ms": ext_ms, "algorithmic_bytes": ext_bytes,
                                 "achieved": ext_bytes / (ext_ms * 1e-3) / 1e9, "peak": smem_peak, "unit": "GB/s",
                                 "frac": ext_bytes / (ext_ms * 1e-3) / 1e9 / smem_peak,
-                                "bytes_note": "N/30 B of bitmap reads + 24 B (three 32-bit RMWs) per prime",
+                                "bytes_note": "2 N/30 B of bitmap reads + 8 B (one 32-bit RMW) per prime + 64 RMWs per 1001 words",
                                 "phases": "last-prime scan, in-order walk with counters, tile reduce"},
                 }
             elif sp:

@@ -18,11 +18,12 @@
 //                                                            multiples across the tile's span;
 //   3. restore:  sets the bits of base primes lying in the tile (the reference starts each prime
 //                at p^2, :452-466; here the p*1 hit is undone instead);
-//   4. extract:  each thread walks a contiguous chunk of words in order (ffs), its predecessor
-//                prime coming from a block-wide max-scan of the chunks' last primes, and updates
-//                shared-memory counters: the gap histogram (:278-280), the per-residue gap
-//                histogram (:282-287), residue classes for mod-4 and mod-q (:181-232), the
-//                large-gap list (:289-299) and the tile's maximal gap.  Primes never reach HBM.
+//   4. extract:  the residue classes for mod-4 and mod-q (:181-232) are counted by word (all
+//                words w = c mod 1001 share their class slots); then each thread walks an equal
+//                share of the tile's primes in order (ffs), its predecessor prime coming from a
+//                block-wide max-scan of the chunks' last primes, and updates shared-memory
+//                counters: the gap histogram (:278-280), the per-residue gap histogram (:282-287),
+//                the large-gap list (:289-299) and the tile's maximal gap.  Primes never reach HBM.
 // The gaps across tile seams are added by stitch_kernel; reduce_kernel gives each interval its
 // first/last prime and maximal gap.
 #include <cuda_runtime.h>
@@ -300,6 +301,114 @@ __device__ __forceinline__ void clear_wheel_walk(uint32_t* bm, uint32_t p, uint3
 __device__ __forceinline__ void sm_add(uint32_t* cnt, uint32_t idx, uint32_t* err) {
   VOSS_SM_GUARD(idx, (uint32_t)kSmCounters)
   atomicAdd(cnt + idx, 1u);
+}
+
+__device__ __forceinline__ void sm_add_n(uint32_t* cnt, uint32_t idx, uint32_t v, uint32_t* err) {
+  VOSS_SM_GUARD(idx, (uint32_t)kSmCounters)
+  atomicAdd(cnt + idx, v);
+}
+
+// Carry-save adder over bit planes: l = a ^ b ^ c, h = majority(a, b, c).
+__device__ __forceinline__ void csa(uint32_t& h, uint32_t& l, uint32_t a, uint32_t b, uint32_t c) {
+  const uint32_t u = a ^ b;
+  h = (a & b) | (u & c);
+  l = u ^ c;
+}
+
+// Swaps the bits of x selected by mask << s with the bits of y selected by mask (one step of an
+// 8x8 bit-matrix transpose applied to the four byte lanes at once).
+__device__ __forceinline__ void swap_bits(uint32_t& x, uint32_t& y, uint32_t mask, uint32_t s) {
+  const uint32_t t = ((x >> s) ^ y) & mask;
+  y ^= t;
+  x ^= t << s;
+}
+
+// The residue-class counters of a tile's primes (k mod 28 and k mod 143 by wheel residue: every
+// q of the reference's mod-4 and mod-q counts, voss_v7_live.cu:181-232), counted by word instead of
+// by prime.  The slots of bit b of word w are 8 ((k28 + 4w) mod 28) + b and 8 ((k143 + 4w) mod
+// 143) + b, and 4004 = 4 * 1001 is a multiple of 28 and of 143, so all words w = c (mod 1001) share
+// their 32 slots in each block.  A thread takes the words of one class c and adds them column by
+// column into six bit planes with carry-save adders (a column counts at most 63 words; a tile of at
+// most 53 KB words gives a class at most 53), transposes the planes into 32 byte-sized column
+// counts and adds each column to its two slots: 64 shared-memory atomics per class instead of two
+// per prime.  The planes are first rotated by the lane number, so lane l adds column (s + l) mod 32
+// at step s: the k mod 28 slots of a warp then lie in 32 distinct banks (8 (k28 + 4w) mod 32 is
+// the same for every w), and the k mod 143 slots as well once each lane's bytes are shifted by its
+// own (k143 + 4c) mod 4.
+template <int BLOCK>
+__device__ __forceinline__ void class_counts_by_word(const uint32_t* bm, uint32_t nw, uint32_t k28,
+                                                     uint32_t k143, uint32_t* cnt, uint32_t lane,
+                                                     uint32_t* err) {
+  for (uint32_t c = threadIdx.x; c < 1001u; c += BLOCK) {
+    uint32_t p0 = 0, p1 = 0, p2 = 0, p3 = 0, p4 = 0, p5 = 0;
+    uint32_t w = c;
+    for (; w + 7u * 1001u < nw; w += 8u * 1001u) {  // eight words: three levels of adders
+      uint32_t a1, a2, a3, a4, b1, b2, c1;
+      csa(a1, p0, p0, bm[w], bm[w + 1001u]);
+      csa(a2, p0, p0, bm[w + 2u * 1001u], bm[w + 3u * 1001u]);
+      csa(b1, p1, p1, a1, a2);
+      csa(a3, p0, p0, bm[w + 4u * 1001u], bm[w + 5u * 1001u]);
+      csa(a4, p0, p0, bm[w + 6u * 1001u], bm[w + 7u * 1001u]);
+      csa(b2, p1, p1, a3, a4);
+      csa(c1, p2, p2, b1, b2);
+      const uint32_t t3 = p3 & c1;
+      p3 ^= c1;
+      p5 ^= p4 & t3;
+      p4 ^= t3;
+    }
+    for (; w < nw; w += 1001u) {  // the rest one word at a time
+      const uint32_t x = bm[w];
+      const uint32_t t0 = p0 & x;
+      p0 ^= x;
+      const uint32_t t1 = p1 & t0;
+      p1 ^= t0;
+      const uint32_t t2 = p2 & t1;
+      p2 ^= t1;
+      const uint32_t t3 = p3 & t2;
+      p3 ^= t2;
+      p5 ^= p4 & t3;
+      p4 ^= t3;
+    }
+    // rotate: bit s of each plane becomes column (s + lane) mod 32
+    p0 = __funnelshift_r(p0, p0, lane);
+    p1 = __funnelshift_r(p1, p1, lane);
+    p2 = __funnelshift_r(p2, p2, lane);
+    p3 = __funnelshift_r(p3, p3, lane);
+    p4 = __funnelshift_r(p4, p4, lane);
+    p5 = __funnelshift_r(p5, p5, lane);
+    // transpose each byte lane's 8x8 bit matrix (planes 6 and 7 are zero): afterwards byte n of
+    // t_j is the count of rotated column 8n + j
+    uint32_t t0 = p0, t1 = p1, t2 = p2, t3 = p3, t4 = p4, t5 = p5, t6 = 0, t7 = 0;
+    swap_bits(t0, t4, 0x0F0F0F0Fu, 4);
+    swap_bits(t1, t5, 0x0F0F0F0Fu, 4);
+    swap_bits(t2, t6, 0x0F0F0F0Fu, 4);
+    swap_bits(t3, t7, 0x0F0F0F0Fu, 4);
+    swap_bits(t0, t2, 0x33333333u, 2);
+    swap_bits(t1, t3, 0x33333333u, 2);
+    swap_bits(t4, t6, 0x33333333u, 2);
+    swap_bits(t5, t7, 0x33333333u, 2);
+    swap_bits(t0, t1, 0x55555555u, 1);
+    swap_bits(t2, t3, 0x55555555u, 1);
+    swap_bits(t4, t5, 0x55555555u, 1);
+    swap_bits(t6, t7, 0x55555555u, 1);
+    const uint32_t tt[8] = {t0, t1, t2, t3, t4, t5, t6, t7};
+    const uint32_t u28 = (k28 + 4u * c) % 28u, u143 = (k143 + 4u * c) % 143u;
+    const uint32_t base28 = (uint32_t)kSmCls28 + 8u * u28, base143 = (uint32_t)kSmCls143 + 8u * u143;
+    // k mod 143 slots: byte n of the step's word is taken from byte (n - m) mod 4, m = u143 mod 4,
+    // so that lane l adds column (s + l - 8m) mod 32 there
+    const uint32_t m = u143 & 3u;
+    const uint32_t r143 = (lane - 8u * m) & 31u;
+    uint32_t sel[4];
+#pragma unroll
+    for (uint32_t n = 0; n < 4; ++n) sel[n] = 0x4440u | ((n - m) & 3u);
+#pragma unroll
+    for (uint32_t s = 0; s < 32; ++s) {
+      const uint32_t v28 = (tt[s & 7u] >> (8u * (s >> 3))) & 0xFFu;
+      const uint32_t v143 = __byte_perm(tt[s & 7u], 0u, sel[s >> 3]);
+      sm_add_n(cnt, base28 + ((s + lane) & 31u), v28, err);
+      sm_add_n(cnt, base143 + ((s + r143) & 31u), v143, err);
+    }
+  }
 }
 
 // Mask of the bits of word w whose integers lie in [vlo, vhi); v0 = value of byte 4w, residue 0.
@@ -866,6 +975,7 @@ sieve_tiles_kernel(SieveArgs a) {
       }
       __syncthreads();
     } else {
+      class_counts_by_word<BLOCK>(bm, nw, H.k28, H.k143, cnt, (uint32_t)lane, err);
       // pass 1: the primes of my chunk and its last prime
       uint32_t pc = 0;
       int32_t my_last = -1;
@@ -935,13 +1045,8 @@ sieve_tiles_kernel(SieveArgs a) {
           }
         }
       }
-      // The class counters of a word's 4 bytes are indexed without wrapping (k mod 28 + j up to
-      // 30, k mod 143 + j up to 145: 31 and 146 classes); the flush folds the tail classes back.
-      // That makes both class indices one add per prime.
       const uint32_t vb = H.vb;
       const uint32_t cthr = H.cthr;
-      uint32_t c28 = (uint32_t)kSmCls28 + 8u * ((H.k28 + 4u * w) % 28u);
-      uint32_t c143 = (uint32_t)kSmCls143 + 8u * ((H.k143 + 4u * w) % 143u);
       uint32_t mg = 0, mlo = 0;
       uint32_t o_prev = 0;  // wheel residue of the previous prime (modq counters: 8 * (g / 2) + o)
       if (prev >= 0) {
@@ -955,16 +1060,10 @@ sieve_tiles_kernel(SieveArgs a) {
         while (x == 0u) {
           x = bm[++w];
           wpos += 120u;
-          c28 += 32u;
-          if (c28 >= (uint32_t)kSmCls28 + 224u) c28 -= 224u;
-          c143 += 32u;
-          if (c143 >= (uint32_t)kSmCls143 + 1144u) c143 -= 1144u;
         }
         const uint32_t b = (uint32_t)__ffs(x) - 1u;
         x &= x - 1u;
         const uint32_t pos = wpos + s_pos[b];
-        sm_add(cnt, c28 + b, err);
-        sm_add(cnt, c143 + b, err);
         H.first = pos;
         prev = (int32_t)pos;
         o_prev = b & 7u;
@@ -981,16 +1080,10 @@ sieve_tiles_kernel(SieveArgs a) {
           while (x == 0u) {  // the tile holds rb >= ra + it + 1 primes: w stays inside it
             x = bm[++w];
             wpos += 120u;
-            c28 += 32u;
-            if (c28 >= (uint32_t)kSmCls28 + 224u) c28 -= 224u;
-            c143 += 32u;
-            if (c143 >= (uint32_t)kSmCls143 + 1144u) c143 -= 1144u;
           }
           const uint32_t b = (uint32_t)__ffs(x) - 1u;
           x &= x - 1u;
           const uint32_t pos = wpos + s_pos[b];
-          sm_add(cnt, c28 + b, err);
-          sm_add(cnt, c143 + b, err);
           const uint32_t g = pos - pv;
           const bool crossing = kCross && (pv < vb) && (pos >= vb);
           const bool small = g < 100u && !crossing;

@@ -301,24 +301,46 @@ def mr_mulmods(sample) -> tuple[int, int]:
 
 
 # ---------------------------------------------------------------------------------------
+def sample_slices(n: int, span: int, k: int = 8) -> list[tuple[int, int]]:
+    """A stratified sample of [1, n]: k slices of span/k integers, slice j centred in the j-th of
+    k equal parts, so the sample's rate is that of the whole range (the CPU sieve slows as the
+    base primes grow towards isqrt(n))."""
+    w = max(1, span // k)
+    out = []
+    for j in range(k):
+        c = 1 + (2 * j + 1) * n // (2 * k)
+        lo = max(1, min(c - w // 2, n + 1 - w))
+        out.append((lo, lo + w))
+    return out
+
+
+def time_slices(slices, threads: int) -> float:
+    import oracle_lib as O
+    t0 = time.perf_counter()
+    for lo, hi in slices:
+        O.sieve_range(lo, hi, compat=True, seg_num=SEG_NUM, threads=threads)
+    return time.perf_counter() - t0
+
+
+def describe_slices(slices) -> str:
+    w = slices[0][1] - slices[0][0]
+    return (f"{len(slices)} slices of {w:.3e} integers centred in the {len(slices)} equal parts of the range "
+            f"(first [{slices[0][0]}, {slices[0][1]}), last [{slices[-1][0]}, {slices[-1][1]}))")
+
+
 def cpu_baseline(n: int, seconds: float, ranges_done=None) -> dict:
-    """Oracle OpenMP interval sieve (port of verify_cpp's marking loop) on the top of [1, n]."""
+    """Oracle OpenMP interval sieve (port of verify_cpp's marking loop) on a stratified sample of
+    [1, n] sized to about `seconds` of CPU work."""
     import oracle_lib as O
     threads = O.oracle().oracle_max_threads()
-    probe = 2 * 10**8
-    lo = max(1, n + 1 - probe)
-    t0 = time.perf_counter()
-    O.sieve_range(lo, n + 1, compat=True, seg_num=SEG_NUM, threads=threads)
-    dt = time.perf_counter() - t0
-    rate = (n + 1 - lo) / max(dt, 1e-6)
-    span = int(min(n, max(probe, rate * seconds)))
-    lo = max(1, n + 1 - span)
-    t0 = time.perf_counter()
-    O.sieve_range(lo, n + 1, compat=True, seg_num=SEG_NUM, threads=threads)
-    dt = time.perf_counter() - t0
-    return {"value": (n + 1 - lo) / dt, "unit": "range/s", "cores": threads, "kind": "port",
-            "sample": f"oracle interval sieve + statistics of [{lo}, {n}] ({n + 1 - lo:.3e} integers, "
-                      f"{dt:.1f} s, OpenMP {threads} threads)"}
+    probe = sample_slices(n, 2 * 10**8)
+    rate = sum(h - l for l, h in probe) / max(time_slices(probe, threads), 1e-6)
+    sl = sample_slices(n, int(min(n, max(2 * 10**8, rate * seconds))))
+    dt = time_slices(sl, threads)
+    total = sum(h - l for l, h in sl)
+    return {"value": total / dt, "unit": "range/s", "cores": threads, "kind": "port",
+            "sample": f"oracle interval sieve + statistics, {describe_slices(sl)}, {total:.3e} integers, "
+                      f"{dt:.1f} s, OpenMP {threads} threads"}
 
 
 def ref_cuda_baseline(n: int) -> dict | None:
@@ -350,24 +372,17 @@ def run_reference_arm(a) -> None:
         return
     import oracle_lib as O
     threads = O.oracle().oracle_max_threads()
-    # size one step as a bounded sample (about 4 s) of the top of [1, n]
-    probe = 10**8
-    lo = a.n + 1 - probe
-    t0 = time.perf_counter()
-    O.sieve_range(lo, a.n + 1, compat=True, seg_num=SEG_NUM, threads=threads)
-    rate = probe / (time.perf_counter() - t0)
-    span = int(min(a.n, max(probe, rate * 4.0)))
-    lo = a.n + 1 - span
+    # one step = a bounded stratified sample (about 4 s of CPU work) of [1, n]
+    probe = sample_slices(a.n, 10**8)
+    rate = sum(h - l for l, h in probe) / max(time_slices(probe, threads), 1e-6)
+    sl = sample_slices(a.n, int(min(a.n, max(10**8, rate * 4.0))))
+    span = sum(h - l for l, h in sl)
     for _ in range(a.warmup):
-        O.sieve_range(lo, a.n + 1, compat=True, seg_num=SEG_NUM, threads=threads)
-    times = []
-    for _ in range(a.steps):
-        t0 = time.perf_counter()
-        O.sieve_range(lo, a.n + 1, compat=True, seg_num=SEG_NUM, threads=threads)
-        times.append(time.perf_counter() - t0)
+        time_slices(sl, threads)
+    times = [time_slices(sl, threads) for _ in range(a.steps)]
     ms = 1e3 * statistics.mean(times)
     value = span / (ms * 1e-3)
-    sample = f"oracle interval sieve + statistics of [{lo}, {a.n}] per step ({span:.3e} integers)"
+    sample = f"oracle interval sieve + statistics per step: {describe_slices(sl)} ({span:.3e} integers)"
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "range/s", "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",

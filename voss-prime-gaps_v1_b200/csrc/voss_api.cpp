@@ -346,8 +346,8 @@ int launch_plan(voss_ctx* c, const RunPlan& P, bool want_large, uint64_t large_c
 
 // memcpy split over host threads: one thread copies from pageable memory at a fraction of the
 // host's memory bandwidth.  A part whose thread cannot be started is copied by the caller.
-void parallel_copy(void* dst, const void* src, size_t bytes) {
-  const size_t kMinPart = 8u << 20;
+void parallel_copy(void* dst, const void* src, size_t bytes, size_t min_part) {
+  const size_t kMinPart = min_part;
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
   const size_t parts = std::min<size_t>({(size_t)std::min(hw, 8u), bytes / kMinPart + 1});
   if (parts <= 1) {
@@ -367,6 +367,43 @@ void parallel_copy(void* dst, const void* src, size_t bytes) {
     }
   }
   std::memcpy(dst, src, std::min(bytes, step));
+  for (auto& t : th) t.join();
+}
+
+// Copies the segments one after another into dst, the concatenated bytes split evenly over up to
+// 8 host threads (parts of at least min_part bytes).  A part whose thread cannot be started is
+// copied by the caller.
+void parallel_gather(void* dst, const CopySeg* seg, size_t n_seg, size_t min_part) {
+  size_t total = 0;
+  for (size_t i = 0; i < n_seg; ++i) total += seg[i].bytes;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t parts = std::min<size_t>({(size_t)std::min(hw, 8u), total / std::max<size_t>(min_part, 1) + 1});
+  auto copy_range = [=](size_t a, size_t b) {  // bytes [a, b) of the concatenation
+    size_t pos = 0;
+    for (size_t i = 0; i < n_seg && pos < b; ++i) {
+      const size_t s0 = pos, s1 = pos + seg[i].bytes;
+      pos = s1;
+      const size_t x = std::max(a, s0), y = std::min(b, s1);
+      if (x < y) std::memcpy((char*)dst + x, (const char*)seg[i].src + (x - s0), y - x);
+    }
+  };
+  if (parts <= 1) {
+    copy_range(0, total);
+    return;
+  }
+  const size_t step = (total / parts + 63) & ~(size_t)63;
+  std::vector<std::thread> th;
+  th.reserve(parts);
+  for (size_t i = 1; i < parts; ++i) {
+    const size_t a = std::min(total, i * step), b = std::min(total, (i + 1) * step);
+    if (a >= b) continue;
+    try {
+      th.emplace_back(copy_range, a, b);
+    } catch (const std::exception&) {
+      copy_range(a, b);
+    }
+  }
+  copy_range(0, std::min(total, step));
   for (auto& t : th) t.join();
 }
 

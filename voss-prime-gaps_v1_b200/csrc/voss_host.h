@@ -167,6 +167,14 @@ void route_intervals(const voss_ctx* c, const uint64_t* lo, const uint64_t* hi, 
 int launch_routed(voss_ctx* c, Workspace& W, const LaunchEvents& E, const IntervalRoute& R, uint32_t n,
                   cudaStream_t s, uint32_t* kernels);
 int check_device_error(const uint32_t* ctr_host);
+// memcpy split over up to 8 host threads, in parts of at least min_part bytes.
+void parallel_copy(void* dst, const void* src, size_t bytes, size_t min_part = 8u << 20);
+struct CopySeg {
+  const void* src;
+  size_t bytes;
+};
+// The segments copied back to back into dst, split the same way.
+void parallel_gather(void* dst, const CopySeg* seg, size_t n_seg, size_t min_part);
 std::vector<uint64_t> small_primes_in(uint64_t lo, uint64_t hi);
 // Add the primes 2, 3, 5 of [lo, hi) to a device-finalized interval result.
 void add_small_primes(voss_interval_stats& st, uint64_t lo, uint64_t hi);

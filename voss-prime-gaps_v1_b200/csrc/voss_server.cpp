@@ -19,6 +19,7 @@
 #include <deque>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -35,12 +36,17 @@ using Clock = std::chrono::steady_clock;
 
 enum ReqState { kPending = 1, kRunning = 2, kDone = 0 };
 
+// Candidate payloads are copied by up to 8 host threads in parts of at least 1 MB: one thread
+// copies at a fraction of the host's memory bandwidth, and a thread costs tens of microseconds.
+constexpr size_t kCopyPart = 1u << 20;
+
 struct Request {
   uint64_t id = 0;
   int kind = 0;  // 0: interval, 1: Miller-Rabin
   uint64_t lo = 0, hi = 0;
   uint32_t tiles = 0;
-  std::vector<uint64_t> in;
+  std::unique_ptr<uint64_t[]> in;  // Miller-Rabin candidates (not zero-filled before the copy)
+  uint64_t n_in = 0;
   std::vector<uint8_t> out;
   voss_interval_stats st;
   Clock::time_point t_submit, t_start, t_done;
@@ -143,11 +149,15 @@ int launch_batch(voss_server* S, Slot& sl) {
   } else {
     std::memset(sl.h_ctr, 0, sizeof(uint32_t) * kCtrWords);
   }
+  // the batch's candidates into the slot's pinned staging, split over host threads
   sl.n_mr = 0;
+  std::vector<CopySeg> segs;
+  segs.reserve(sl.mr.size());
   for (Request* r : sl.mr) {
-    std::memcpy(sl.h_mr_in + sl.n_mr, r->in.data(), r->in.size() * 8);
-    sl.n_mr += r->in.size();
+    segs.push_back(CopySeg{r->in.get(), r->n_in * 8});
+    sl.n_mr += r->n_in;
   }
+  parallel_gather(sl.h_mr_in, segs.data(), segs.size(), kCopyPart);
   if (sl.n_mr) {
     CUDA_TRY(cudaMemcpyAsync(sl.ws.mr_in.p, sl.h_mr_in, sl.n_mr * 8, cudaMemcpyHostToDevice, s));
     uint32_t* work = sl.ws.mr_work.as<uint32_t>();
@@ -180,10 +190,10 @@ void complete_slot(voss_server* S, Slot& sl) {
   uint64_t off = 0;
   for (Request* r : sl.mr) {
     if (!err) {
-      r->out.resize(r->in.size());
-      std::memcpy(r->out.data(), sl.h_mr_out + off, r->in.size());
+      r->out.resize(r->n_in);
+      std::memcpy(r->out.data(), sl.h_mr_out + off, r->n_in);
     }
-    off += r->in.size();
+    off += r->n_in;
     r->error = err;
     r->state = kDone;
     r->t_done = now;
@@ -212,8 +222,8 @@ bool form_batch(voss_server* S, Slot& sl) {
       tiles += r->tiles;
       sl.iv.push_back(r);
     } else {
-      if (cand + r->in.size() > S->cfg.max_batch_candidates) break;
-      cand += r->in.size();
+      if (cand + r->n_in > S->cfg.max_batch_candidates) break;
+      cand += r->n_in;
       sl.mr.push_back(r);
     }
     r->state = kRunning;
@@ -421,7 +431,12 @@ VOSS_API int voss_server_submit_mr(voss_server* S, const uint64_t* n, uint64_t c
                 (unsigned long long)S->cfg.max_batch_candidates);
   auto r = std::make_unique<Request>();
   r->kind = 1;
-  r->in.assign(n, n + count);
+  r->n_in = count;
+  if (count) {
+    r->in.reset(new (std::nothrow) uint64_t[count]);
+    if (!r->in) return fail(VOSS_ERR_NOMEM, "no host memory for %llu candidates", (unsigned long long)count);
+    parallel_copy(r->in.get(), n, count * 8, kCopyPart);
+  }
   *ticket = enqueue(S, std::move(r));
   return VOSS_OK;
 }

@@ -324,17 +324,17 @@ __device__ __forceinline__ void swap_bits(uint32_t& x, uint32_t& y, uint32_t mas
 }
 
 // The residue-class counters of a tile's primes (k mod 28 and k mod 143 by wheel residue: every
-// q of the reference's mod-4 and mod-q counts, voss_v7_live.cu:181-232), counted by word instead of
-// by prime.  The slots of bit b of word w are 8 ((k28 + 4w) mod 28) + b and 8 ((k143 + 4w) mod
-// 143) + b, and 4004 = 4 * 1001 is a multiple of 28 and of 143, so all words w = c (mod 1001) share
-// their 32 slots in each block.  A thread takes the words of one class c and adds them column by
-// column into six bit planes with carry-save adders (a column counts at most 63 words; a tile of at
-// most 53 KB words gives a class at most 53), transposes the planes into 32 byte-sized column
-// counts and adds each column to its two slots: 64 shared-memory atomics per class instead of two
-// per prime.  The planes are first rotated by the lane number, so lane l adds column (s + l) mod 32
-// at step s: the k mod 28 slots of a warp then lie in 32 distinct banks (8 (k28 + 4w) mod 32 is
-// the same for every w), and the k mod 143 slots as well once each lane's bytes are shifted by its
-// own (k143 + 4c) mod 4.
+// q of the reference's mod-4 and mod-q counts, voss_v7_live.cu:181-232), counted by word instead
+// of by prime.  The slots of bit b of word w are 8 ((k28 + 4w) mod 28) + b and
+// 8 ((k143 + 4w) mod 143) + b, and 4004 = 4 * 1001 is a multiple of 28 and of 143, so all words
+// w = c (mod 1001) share their 32 slots in each block.  A thread takes the words of one class c
+// and adds them column by column into six bit planes with carry-save adders (a column counts at
+// most 63 words; shared memory holds tiles of at most about 52,000 words, at most 52 per class),
+// transposes the planes into 32 byte-sized column counts and adds each column to its two slots:
+// 64 shared-memory atomics per class instead of two per prime.  The planes are first rotated by
+// the lane number, so lane l adds column (s + l) mod 32 at step s: the k mod 28 slots of a warp
+// then lie in 32 distinct banks (8 (k28 + 4w) mod 32 is the same for every w), and the k mod 143
+// slots as well once each lane's bytes are shifted by its own (k143 + 4c) mod 4.
 template <int BLOCK>
 __device__ __forceinline__ void class_counts_by_word(const uint32_t* bm, uint32_t nw, uint32_t k28,
                                                      uint32_t k143, uint32_t* cnt, uint32_t lane,

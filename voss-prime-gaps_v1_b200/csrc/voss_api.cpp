@@ -133,7 +133,7 @@ int apply_tuning(voss_ctx* c, const voss_tuning& t0) {
     return fail(VOSS_ERR_ARG, "chunk_words must be odd and <= 255");
   const uint32_t tw = t.block_threads * t.chunk_words;
   // the tile kernel counts residue classes over the words w = c (mod 1001) of a tile in 6-bit
-  // column counters: at most 63 such words (shared memory caps tiles near 57,000 words anyway)
+  // column counters: at most 63 such words (shared memory caps tiles near 52,000 words anyway)
   if (tw > 63u * 1001u) return fail(VOSS_ERR_ARG, "tile of %u words exceeds 63063 words", tw);
   const size_t smem = sieve_smem_bytes(tw);
   int maxc = 0;

@@ -149,6 +149,21 @@ def test_bench_mr_products_small_cases():
     assert s == 0 and f > 0
 
 
+@pytest.mark.parametrize("n,span", [(10**12, 4 * 10**9), (10**12, 10**8), (10**9, 10**9), (1000, 5000), (100, 7)])
+def test_bench_cpu_sample_is_stratified_over_the_range(n, span):
+    """The CPU baseline's sample: 8 equal slices inside [1, n + 1), one centred in each eighth."""
+    bench = _bench()
+    sl = bench.sample_slices(n, span)
+    assert len(sl) == 8
+    widths = {hi - lo for lo, hi in sl}
+    assert len(widths) == 1 and widths.pop() == max(1, span // 8)
+    for j, (lo, hi) in enumerate(sl):
+        assert 1 <= lo < hi <= n + 1
+        if span // 8 <= n // 8:  # a slice fits its eighth: it lies around the eighth's middle
+            assert lo <= 1 + (2 * j + 1) * n // 16 < hi or hi - lo == 1
+    assert [lo for lo, _ in sl] == sorted(lo for lo, _ in sl)
+
+
 @pytest.mark.parametrize("lo,hi,compat,seg", [
     (1, 20000, True, 30), (1, 20000, True, 330), (1, 50000, True, 30_000_000_000),
     (1, 20000, False, 0), (2, 3, False, 0), (0, 8, False, 0), (9000, 31000, False, 0),

@@ -3,7 +3,8 @@
 // The reference has no serving mode.  Requests (interval sieve + gap statistics, or a batch of
 // Miller-Rabin candidates) are queued by any number of client threads.  One scheduler thread owns
 // K "slots"; each slot is a CUDA stream with its own device workspace and pinned host staging,
-// all sized at creation so that serving never allocates.  Whenever a slot is free and requests
+// all sized at creation so that batches never allocate device or pinned memory (a Miller-Rabin
+// request keeps a host copy of its candidates until it is released).  Whenever a slot is free and requests
 // are pending, the scheduler takes the pending requests in arrival order until the slot's
 // capacity (requests, tiles = bitmap memory, candidates) is reached and launches them as one
 // batch: one persistent tile-kernel launch over all the batch's (interval, tile) work items,

@@ -298,7 +298,8 @@ VOSS_API int voss_server_create(voss_ctx* ctx, const voss_server_config* cfg, vo
 VOSS_API void voss_server_destroy(voss_server* srv);
 /* Queue [lo, hi); the answer is a voss_interval_stats equal to voss_sieve_intervals on it alone. */
 VOSS_API int voss_server_submit_interval(voss_server* srv, uint64_t lo, uint64_t hi, uint64_t* ticket);
-/* Queue Miller-Rabin verdicts for n[0..count) (copied at submission). */
+/* Queue Miller-Rabin verdicts for n[0..count) (copied at submission, by up to 8 host threads for
+ * large batches; VOSS_ERR_NOMEM when the host copy cannot be allocated). */
 VOSS_API int voss_server_submit_mr(voss_server* srv, const uint64_t* n, uint64_t count, uint64_t* ticket);
 /* VOSS_OK once the request finished, VOSS_ERR_TIMEOUT after timeout_ms, or the request's error. */
 VOSS_API int voss_server_wait(voss_server* srv, uint64_t ticket, uint32_t timeout_ms);

@@ -328,7 +328,7 @@ def describe_slices(slices) -> str:
             f"(first [{slices[0][0]}, {slices[0][1]}), last [{slices[-1][0]}, {slices[-1][1]}))")
 
 
-def cpu_baseline(n: int, seconds: float, ranges_done=None) -> dict:
+def cpu_baseline(n: int, seconds: float) -> dict:
     """Oracle OpenMP interval sieve (port of verify_cpp's marking loop) on a stratified sample of
     [1, n] sized to about `seconds` of CPU work."""
     import oracle_lib as O
